@@ -1,0 +1,756 @@
+// Host side of the BLR-LU engine: plan allocation, the per-step driver of the
+// factorization (captured once into a CUDA graph and replayed), block
+// substitution, the FP64 H-matvec, iterative refinement and the C ABI
+// declared in include/frank_b200.h.
+#include "blr_kernels.cuh"
+#include "../../include/frank_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace frank;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                      \
+  do {                                                                                      \
+    cudaError_t _e = (expr);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      return fail(FRANK_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));      \
+  } while (0)
+
+template <typename P>
+cudaError_t dalloc(P** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(P));
+}
+
+}  // namespace
+
+struct frank_blr {
+  int64_t n = 0;
+  int nb = 0, bmax = 0, kcap = 0, precision = 0, fixed_rank = 0;
+  double eps = 0.0, admis = 0.0;
+  int device = 0, sm_count = 0;
+  std::vector<int> off_h, dslot_h, lslot_h;
+  int ndense = 0, nlr = 0;
+  bool dense_offdiag = false;
+  // device geometry
+  int *d_off = nullptr, *d_dslot = nullptr, *d_lslot = nullptr;
+  int *d_rankH = nullptr, *d_rankW = nullptr;
+  // A_H (FP64)
+  double *Hd = nullptr, *Hu = nullptr, *Hs = nullptr, *Hv = nullptr;
+  // working copy (T)
+  void *Wd = nullptr, *Wu = nullptr, *Ws = nullptr, *Wv = nullptr;
+  // factor workspace
+  int *perm = nullptr, *ipiv = nullptr, *err = nullptr;
+  void *Linv = nullptr, *Uinv = nullptr, *WL = nullptr, *WU = nullptr;
+  double *getrf_scratch = nullptr, *dscratch = nullptr, *rscratch = nullptr;
+  int64_t dstride = 0, rstride = 0;
+  int grid_dense = 0, grid_recomp = 0, smax = 0;
+  // solve / matvec temporaries (nrhs <= 8 per pass)
+  void* z = nullptr;         // n x 8 (T)
+  void* stmp = nullptr;      // bmax x 8 (T)
+  void* sctmp = nullptr;     // nb x bmax x 8 (T)
+  double* part = nullptr;    // nb*nb x bmax x 8
+  double* vtmp = nullptr;    // n x 8 x 3 (residual, correction, rhs copy)
+  double* nrm = nullptr;     // norm partials
+  double* nrm_h = nullptr;   // pinned host mirror
+  int nrm_blocks = 0;
+  // state
+  bool factored = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  int64_t launches = 0;
+  int err_h[ERR_SLOTS] = {0};
+};
+
+namespace {
+
+template <typename T>
+BlrView<T> work_view(frank_blr* p) {
+  BlrView<T> v;
+  v.nb = p->nb; v.bmax = p->bmax; v.kcap = p->kcap;
+  v.off = p->d_off; v.dslot = p->d_dslot; v.lslot = p->d_lslot; v.rank = p->d_rankW;
+  v.D = static_cast<T*>(p->Wd); v.U = static_cast<T*>(p->Wu);
+  v.S = static_cast<T*>(p->Ws); v.Vt = static_cast<T*>(p->Wv);
+  return v;
+}
+
+BlrView<double> h_view(const frank_blr* p) {
+  BlrView<double> v;
+  v.nb = p->nb; v.bmax = p->bmax; v.kcap = p->kcap;
+  v.off = p->d_off; v.dslot = p->d_dslot; v.lslot = p->d_lslot; v.rank = p->d_rankH;
+  v.D = p->Hd; v.U = p->Hu; v.S = p->Hs; v.Vt = p->Hv;
+  return v;
+}
+
+template <typename T>
+FactorWs<T> factor_ws(frank_blr* p) {
+  FactorWs<T> w;
+  w.perm = p->perm; w.ipiv = p->ipiv;
+  w.Linv = static_cast<T*>(p->Linv); w.Uinv = static_cast<T*>(p->Uinv);
+  w.WL = static_cast<T*>(p->WL); w.WU = static_cast<T*>(p->WU);
+  w.getrf_scratch = p->getrf_scratch;
+  w.dscratch = p->dscratch; w.dscratch_stride = p->dstride;
+  w.rscratch = p->rscratch; w.rscratch_stride = p->rstride;
+  w.err = p->err; w.fixed_rank = p->fixed_rank; w.eps = p->eps;
+  return w;
+}
+
+size_t tsize(const frank_blr* p) { return p->precision == FRANK_PREC_FP64 ? sizeof(double) : sizeof(float); }
+
+int check_block(const frank_blr* p, int i, int j) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  if (i < 0 || j < 0 || i >= p->nb || j >= p->nb) return fail(FRANK_ERR_INVALID, "block index out of range");
+  return FRANK_OK;
+}
+
+// Enqueue all launches of one factorization on stream s.
+template <typename T>
+int enqueue_factor(frank_blr* p, cudaStream_t s) {
+  BlrView<double> H = h_view(p);
+  BlrView<T> W = work_view<T>(p);
+  FactorWs<T> ws = factor_ws<T>(p);
+  int64_t launches = 0;
+  k_reset<T><<<p->nb * p->nb, 256, 0, s>>>(H, W);
+  ++launches;
+  CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
+  for (int i = 0; i < p->nb; ++i) {
+    k_getrf<T><<<1, GETRF_THREADS, 0, s>>>(W, ws, i);
+    ++launches;
+    const int m = p->nb - i - 1;
+    if (m == 0) break;
+    k_panel<T><<<2 * m, PANEL_THREADS, 0, s>>>(W, ws, i);
+    ++launches;
+    const int mm = m * m;
+    k_update_dense<T><<<std::min(mm, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
+    ++launches;
+    if (p->nlr > 0) {
+      k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, 0, s>>>(W, ws, i, p->smax);
+      ++launches;
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  p->launches = launches;
+  return FRANK_OK;
+}
+
+template <typename T>
+int run_factor(frank_blr* p, cudaStream_t s) {
+  if (!p->graph_exec) {
+    // Capture the whole step sequence once; kernel arguments are fixed
+    // device pointers, ranks are read from device tables at run time.
+    CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_factor<T>(p, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc != FRANK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    p->graph = g;
+    CUDA_TRY(cudaGraphInstantiate(&p->graph_exec, g, 0));
+  }
+  CUDA_TRY(cudaGraphLaunch(p->graph_exec, s));
+  CUDA_TRY(cudaMemcpyAsync(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  p->factored = true;
+  if (p->err_h[ERR_SINGULAR_STEP] != 0) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "zero pivot in the leaf getrf of diagonal block %d", p->err_h[ERR_SINGULAR_STEP] - 1);
+    return fail(FRANK_ERR_SINGULAR, buf);
+  }
+  if (p->err_h[ERR_BOUNDS] != 0) return fail(FRANK_ERR_INVALID, "stacked rank exceeded the recompression scratch");
+  if (p->err_h[ERR_RANK_OVERFLOW] != 0) return fail(FRANK_ERR_RANK_OVERFLOW, "a recompressed rank exceeded max_rank and was clamped");
+  return FRANK_OK;
+}
+
+// ---- solve --------------------------------------------------------------
+
+template <typename T>
+int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cudaStream_t s) {
+  BlrView<T> W = work_view<T>(p);
+  FactorWs<T> ws = factor_ws<T>(p);
+  T* tmp = static_cast<T*>(p->stmp);
+  T* sct = static_cast<T*>(p->sctmp);
+  const size_t shm = (size_t)p->kcap * nrhs * sizeof(double);
+  const int nb = p->nb;
+  if (!transpose) {
+    for (int i = 0; i < nb; ++i) {
+      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 0, tmp);
+      if (nb - i - 1 > 0) k_solve_scatter<T><<<nb - i - 1, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 0, sct);
+    }
+    for (int i = nb - 1; i >= 0; --i) {
+      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 1, tmp);
+      if (i > 0) k_solve_scatter<T><<<i, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 1, sct);
+    }
+  } else {
+    for (int i = 0; i < nb; ++i) {
+      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 2, tmp);
+      if (nb - i - 1 > 0) k_solve_scatter<T><<<nb - i - 1, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 2, sct);
+    }
+    for (int i = nb - 1; i >= 0; --i) {
+      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 3, tmp);
+      if (i > 0) k_solve_scatter<T><<<i, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 3, sct);
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FRANK_OK;
+}
+
+int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 4096); }
+
+// d_b (double, n x nrhs) -> solve in T -> back into d_b.
+int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s) {
+  if (!p->factored) return fail(FRANK_ERR_STATE, "solve before getrf");
+  for (int c0 = 0; c0 < nrhs; c0 += 8) {
+    const int nr = std::min(8, nrhs - c0);
+    double* b = d_b + c0 * ldb;
+    if (p->precision == FRANK_PREC_FP64) {
+      int rc = enqueue_solve<double>(p, b, ldb, nr, transpose, s);
+      if (rc) return rc;
+    } else {
+      float* z = static_cast<float*>(p->z);
+      k_cast_copy<float, double><<<grid_for(p->n * nr), 256, 0, s>>>(b, ldb, z, p->n, p->n, nr);
+      int rc = enqueue_solve<float>(p, z, p->n, nr, transpose, s);
+      if (rc) return rc;
+      k_cast_copy<double, float><<<grid_for(p->n * nr), 256, 0, s>>>(z, p->n, b, ldb, p->n, nr);
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FRANK_OK;
+}
+
+int matvec_device_impl(frank_blr* p, const double* x, int64_t ldx, double* y, int64_t ldy, int nrhs,
+                       const double* bres, int64_t ldb, cudaStream_t s) {
+  BlrView<double> H = h_view(p);
+  for (int c0 = 0; c0 < nrhs; c0 += 8) {
+    const int nr = std::min(8, nrhs - c0);
+    const size_t shm = 2 * (size_t)p->kcap * nr * sizeof(double);
+    k_matvec_blocks<<<dim3(p->nb, p->nb), MV_THREADS, shm, s>>>(H, x + c0 * ldx, ldx, nr, p->part);
+    k_matvec_reduce<<<p->nb, 256, 0, s>>>(H, p->part, nr, bres ? bres + c0 * ldb : nullptr, ldb, y + c0 * ldy, ldy);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FRANK_OK;
+}
+
+// max_j ||v_j|| / ||w_j|| with host reduction of per-CTA partials.
+int colnorms(frank_blr* p, const double* v, int64_t ldv, int nrhs, std::vector<double>& out, cudaStream_t s) {
+  out.assign(nrhs, 0.0);
+  for (int c0 = 0; c0 < nrhs; c0 += 8) {
+    const int nr = std::min(8, nrhs - c0);
+    k_colnorm2<<<p->nrm_blocks, 256, 0, s>>>(v + c0 * ldv, p->n, ldv, nr, p->nrm);
+    CUDA_TRY(cudaMemcpyAsync(p->nrm_h, p->nrm, sizeof(double) * p->nrm_blocks * nr, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    for (int b = 0; b < p->nrm_blocks; ++b)
+      for (int h = 0; h < nr; ++h) out[c0 + h] += p->nrm_h[b * nr + h];
+  }
+  for (auto& v2 : out) v2 = std::sqrt(v2);
+  return FRANK_OK;
+}
+
+int refine_device_impl(frank_blr* p, const double* b, int64_t ldb, double* x, int64_t ldx, int nrhs, double tol,
+                       int maxit, int* iters, double* resid, cudaStream_t s) {
+  if (!p->factored) return fail(FRANK_ERR_STATE, "refine before getrf");
+  if (nrhs > 8) return fail(FRANK_ERR_UNSUPPORTED, "refine takes at most 8 right-hand sides per call");
+  int rc;
+  std::vector<double> bn, rn;
+  if ((rc = colnorms(p, b, ldb, nrhs, bn, s))) return rc;
+  // x0 = (LU)^{-1} b
+  CUDA_TRY(cudaMemcpy2DAsync(x, ldx * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyDeviceToDevice, s));
+  if ((rc = solve_device_impl(p, x, ldx, nrhs, false, s))) return rc;
+  double* r = p->vtmp;  // n x nrhs residual / correction
+  int it = 0;
+  double res = 0.0;
+  for (;;) {
+    if ((rc = matvec_device_impl(p, x, ldx, r, p->n, nrhs, b, ldb, s))) return rc;
+    if ((rc = colnorms(p, r, p->n, nrhs, rn, s))) return rc;
+    res = 0.0;
+    for (int h = 0; h < nrhs; ++h) res = std::max(res, rn[h] / (bn[h] > 0.0 ? bn[h] : 1.0));
+    if (res <= tol || it >= maxit) break;
+    if ((rc = solve_device_impl(p, r, p->n, nrhs, false, s))) return rc;
+    k_axpy_cast<double><<<grid_for(p->n * nrhs), 256, 0, s>>>(r, p->n, x, ldx, p->n, nrhs);
+    ++it;
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters) *iters = it;
+  if (resid) *resid = res;
+  if (res > tol) return fail(FRANK_ERR_NOT_CONVERGED, "refinement reached maxit before the tolerance");
+  return FRANK_OK;
+}
+
+void free_plan(frank_blr* p) {
+  if (!p) return;
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  void* ptrs[] = {p->d_off, p->d_dslot, p->d_lslot, p->d_rankH, p->d_rankW, p->Hd, p->Hu, p->Hs, p->Hv,
+                  p->Wd, p->Wu, p->Ws, p->Wv, p->perm, p->ipiv, p->err, p->Linv, p->Uinv, p->WL, p->WU,
+                  p->getrf_scratch, p->dscratch, p->rscratch, p->z, p->stmp, p->sctmp, p->part, p->vtmp, p->nrm};
+  for (void* q : ptrs) if (q) cudaFree(q);
+  if (p->nrm_h) cudaFreeHost(p->nrm_h);
+  delete p;
+}
+
+}  // namespace
+
+namespace {
+template <typename T>
+void to_double(const std::vector<char>& raw, std::vector<double>& out, size_t count) {
+  out.resize(count);
+  const T* t = reinterpret_cast<const T*>(raw.data());
+  for (size_t e = 0; e < count; ++e) out[e] = double(t[e]);
+}
+
+int fetch(const frank_blr* p, int which, const void* src, size_t count, std::vector<double>& out) {
+  const size_t es = which ? tsize(p) : sizeof(double);
+  std::vector<char> raw(count * es);
+  cudaError_t e = cudaMemcpy(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  if (es == sizeof(double)) to_double<double>(raw, out, count);
+  else to_double<float>(raw, out, count);
+  return FRANK_OK;
+}
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* frank_last_error(void) { return g_last_error.c_str(); }
+
+int frank_device_info(char* name, int name_len, int* sm_count, int* cc_major, int* cc_minor) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+  if (name && name_len > 0) { strncpy(name, prop.name, name_len - 1); name[name_len - 1] = 0; }
+  if (sm_count) *sm_count = prop.multiProcessorCount;
+  if (cc_major) *cc_major = prop.major;
+  if (cc_minor) *cc_minor = prop.minor;
+  return FRANK_OK;
+}
+
+int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
+  if (!d || !out) return fail(FRANK_ERR_INVALID, "null descriptor");
+  *out = nullptr;
+  if (d->n <= 0 || d->nb <= 0 || d->nb > d->n) return fail(FRANK_ERR_INVALID, "need 0 < nb <= n");
+  if (d->precision != FRANK_PREC_FP64 && d->precision != FRANK_PREC_MIXED)
+    return fail(FRANK_ERR_INVALID, "unknown precision");
+  if (d->fixed_rank < 0 || d->eps < 0.0 || (d->fixed_rank == 0 && d->eps <= 0.0))
+    return fail(FRANK_ERR_INVALID, "need fixed_rank > 0 or eps > 0");
+  frank_blr* p = new frank_blr();
+  p->n = d->n; p->nb = d->nb; p->precision = d->precision; p->fixed_rank = d->fixed_rank;
+  p->eps = d->eps; p->admis = d->admis;
+  // IndexRange::split (index_range.cpp:15-24)
+  const int64_t child = (d->n + d->nb - 1) / d->nb;
+  p->off_h.resize(d->nb + 1);
+  for (int i = 0; i < d->nb; ++i) p->off_h[i] = (int)(child * i);
+  p->off_h[d->nb] = (int)d->n;
+  for (int i = 0; i < d->nb; ++i)
+    if (p->off_h[i + 1] - p->off_h[i] <= 0) { delete p; return fail(FRANK_ERR_INVALID, "empty block from the split"); }
+  p->bmax = (int)child;
+  if (p->bmax > 1024) { delete p; return fail(FRANK_ERR_UNSUPPORTED, "block size above 1024"); }
+  p->kcap = d->max_rank > 0 ? std::min(d->max_rank, p->bmax) : p->bmax;
+  if (p->fixed_rank > p->kcap) p->kcap = std::min(p->fixed_rank, p->bmax);
+  const int nb = d->nb;
+  p->dslot_h.assign(nb * nb, -1);
+  p->lslot_h.assign(nb * nb, -1);
+  for (int i = 0; i < nb; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j];
+      const bool adm = (i != j) && (std::abs(i - j) > (int)d->admis) && bi > 1 && bj > 1;
+      if (adm) p->lslot_h[i * nb + j] = p->nlr++;
+      else { p->dslot_h[i * nb + j] = p->ndense++; if (i != j) p->dense_offdiag = true; }
+    }
+  cudaDeviceProp prop;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) { delete p; return fail(FRANK_ERR_CUDA, std::string("device: ") + cudaGetErrorString(e)); }
+  p->device = dev;
+  p->sm_count = prop.multiProcessorCount;
+  const size_t ts = tsize(p);
+  const int64_t bm = p->bmax, kc = p->kcap;
+  p->smax = (int)(kc + (p->dense_offdiag ? bm : kc));
+  const RecompLayout L = recomp_layout(p->bmax, p->smax);
+  p->rstride = L.total;
+  p->dstride = 2 * bm * bm;
+  p->grid_recomp = std::max(1, std::min(nb * nb, 2 * p->sm_count));
+  p->grid_dense = std::max(1, std::min(nb * nb, 2 * p->sm_count));
+  p->nrm_blocks = 256;
+#define ALLOC(ptr, cnt)                                                                   \
+  do {                                                                                    \
+    cudaError_t _e = dalloc(&(ptr), (cnt));                                               \
+    if (_e != cudaSuccess) {                                                              \
+      free_plan(p);                                                                       \
+      return fail(FRANK_ERR_CUDA, std::string("cudaMalloc " #ptr ": ") + cudaGetErrorString(_e)); \
+    }                                                                                     \
+  } while (0)
+  ALLOC(p->d_off, nb + 1);
+  ALLOC(p->d_dslot, nb * nb);
+  ALLOC(p->d_lslot, nb * nb);
+  ALLOC(p->d_rankH, nb * nb);
+  ALLOC(p->d_rankW, nb * nb);
+  ALLOC(p->Hd, p->ndense * bm * bm);
+  ALLOC(p->Hu, p->nlr * bm * kc);
+  ALLOC(p->Hs, p->nlr * kc * kc);
+  ALLOC(p->Hv, p->nlr * bm * kc);
+  char* t;
+  ALLOC(t, p->ndense * bm * bm * ts); p->Wd = t;
+  ALLOC(t, p->nlr * bm * kc * ts); p->Wu = t;
+  ALLOC(t, p->nlr * kc * kc * ts); p->Ws = t;
+  ALLOC(t, p->nlr * bm * kc * ts); p->Wv = t;
+  ALLOC(p->perm, nb * bm);
+  ALLOC(p->ipiv, nb * bm);
+  ALLOC(p->err, ERR_SLOTS);
+  ALLOC(t, nb * bm * bm * ts); p->Linv = t;
+  ALLOC(t, nb * bm * bm * ts); p->Uinv = t;
+  ALLOC(t, nb * bm * bm * ts); p->WL = t;
+  ALLOC(t, nb * bm * bm * ts); p->WU = t;
+  ALLOC(p->getrf_scratch, bm * bm);
+  ALLOC(p->dscratch, (int64_t)p->grid_dense * p->dstride);
+  if (p->nlr > 0) ALLOC(p->rscratch, (int64_t)p->grid_recomp * p->rstride);
+  ALLOC(t, p->n * 8 * ts); p->z = t;
+  ALLOC(t, bm * 8 * ts); p->stmp = t;
+  ALLOC(t, (int64_t)nb * bm * 8 * ts); p->sctmp = t;
+  ALLOC(p->part, (int64_t)nb * nb * bm * 8);
+  ALLOC(p->vtmp, p->n * 8 * 3);
+  ALLOC(p->nrm, p->nrm_blocks * 8);
+#undef ALLOC
+  if (cudaMallocHost(reinterpret_cast<void**>(&p->nrm_h), sizeof(double) * p->nrm_blocks * 8) != cudaSuccess) {
+    free_plan(p);
+    return fail(FRANK_ERR_CUDA, "cudaMallocHost");
+  }
+  std::vector<int> zeros(nb * nb, 0);
+  if (cudaMemcpy(p->d_off, p->off_h.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p->d_dslot, p->dslot_h.data(), sizeof(int) * nb * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p->d_lslot, p->lslot_h.data(), sizeof(int) * nb * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p->d_rankH, zeros.data(), sizeof(int) * nb * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p->d_rankW, zeros.data(), sizeof(int) * nb * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(p->Hd, 0, sizeof(double) * p->ndense * bm * bm) != cudaSuccess) {
+    free_plan(p);
+    return fail(FRANK_ERR_CUDA, "plan upload");
+  }
+  // dynamic shared memory of the solve / matvec kernels (kcap * 8 RHS * 2 doubles)
+  const int shm = (int)(2 * kc * 8 * sizeof(double));
+  cudaFuncSetAttribute(k_matvec_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  cudaFuncSetAttribute(k_solve_scatter<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  *out = p;
+  return FRANK_OK;
+}
+
+int frank_blr_destroy(frank_blr* p) {
+  if (!p) return FRANK_OK;
+  cudaDeviceSynchronize();
+  free_plan(p);
+  return FRANK_OK;
+}
+
+int frank_blr_offsets(const frank_blr* p, int64_t* offsets) {
+  if (!p || !offsets) return fail(FRANK_ERR_INVALID, "null argument");
+  for (int i = 0; i <= p->nb; ++i) offsets[i] = p->off_h[i];
+  return FRANK_OK;
+}
+
+int frank_blr_set_dense(frank_blr* p, int i, int j, const double* a, int64_t ld, int rowmajor) {
+  int rc = check_block(p, i, j);
+  if (rc) return rc;
+  if (!a) return fail(FRANK_ERR_INVALID, "null data");
+  const int s = p->dslot_h[i * p->nb + j];
+  if (s < 0) return fail(FRANK_ERR_INVALID, "block is low rank under the plan's admissibility");
+  const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j];
+  if (ld < (rowmajor ? bj : bi)) return fail(FRANK_ERR_INVALID, "leading dimension too small");
+  std::vector<double> h((size_t)p->bmax * p->bmax, 0.0);
+  for (int c = 0; c < bj; ++c)
+    for (int r = 0; r < bi; ++r) h[r + (size_t)c * p->bmax] = rowmajor ? a[(size_t)r * ld + c] : a[r + (size_t)c * ld];
+  CUDA_TRY(cudaMemcpy(p->Hd + (size_t)s * p->bmax * p->bmax, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  p->factored = false;
+  return FRANK_OK;
+}
+
+int frank_blr_set_lowrank(frank_blr* p, int i, int j, int rank, const double* U, int64_t ldu, const double* S,
+                          int64_t lds, const double* V, int64_t ldv, int rowmajor) {
+  int rc = check_block(p, i, j);
+  if (rc) return rc;
+  const int s = p->lslot_h[i * p->nb + j];
+  if (s < 0) return fail(FRANK_ERR_INVALID, "block is dense under the plan's admissibility");
+  if (rank <= 0 || rank > p->kcap) return fail(FRANK_ERR_RANK_OVERFLOW, "rank outside [1, max_rank]");
+  if (!U || !S || !V) return fail(FRANK_ERR_INVALID, "null data");
+  const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j];
+  const int64_t bm = p->bmax, kc = p->kcap;
+  std::vector<double> hu(bm * kc, 0.0), hs(kc * kc, 0.0), hv(bm * kc, 0.0);
+  for (int c = 0; c < rank; ++c)
+    for (int r = 0; r < bi; ++r) hu[r + c * bm] = rowmajor ? U[(size_t)r * ldu + c] : U[r + (size_t)c * ldu];
+  for (int c = 0; c < rank; ++c)
+    for (int r = 0; r < rank; ++r) hs[r + c * kc] = rowmajor ? S[(size_t)r * lds + c] : S[r + (size_t)c * lds];
+  // V is rank x bj; stored transposed: Vt[col + a*bm] = V(a, col)
+  for (int a = 0; a < rank; ++a)
+    for (int c = 0; c < bj; ++c) hv[c + a * bm] = rowmajor ? V[(size_t)a * ldv + c] : V[a + (size_t)c * ldv];
+  CUDA_TRY(cudaMemcpy(p->Hu + s * bm * kc, hu.data(), hu.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(p->Hs + s * kc * kc, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(p->Hv + s * bm * kc, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(p->d_rankH + i * p->nb + j, &rank, sizeof(int), cudaMemcpyHostToDevice));
+  p->factored = false;
+  return FRANK_OK;
+}
+
+int frank_blr_build_kernel(frank_blr* p, int kernel, const double* points, int dim, const double* kparams,
+                           double eps, void* stream) {
+  if (!p || !points) return fail(FRANK_ERR_INVALID, "null argument");
+  if (kernel < 0 || kernel > 3 || dim < 1 || dim > 3) return fail(FRANK_ERR_INVALID, "bad kernel or dim");
+  if (eps <= 0.0) return fail(FRANK_ERR_UNSUPPORTED, "on-device construction needs eps > 0");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* dx = nullptr;
+  CUDA_TRY(cudaMalloc(&dx, sizeof(double) * dim * p->n));
+  CUDA_TRY(cudaMemcpy(dx, points, sizeof(double) * dim * p->n, cudaMemcpyHostToDevice));
+  KernelDesc K;
+  K.kind = kernel; K.dim = dim; K.x = dx; K.n = p->n;
+  K.p0 = kparams ? kparams[0] : 0.0;
+  K.p1 = kparams ? kparams[1] : 0.0;
+  if (kernel == FRANK_KERNEL_EXP && !(K.p0 > 0.0)) { cudaFree(dx); return fail(FRANK_ERR_INVALID, "exp kernel needs theta > 0"); }
+  std::vector<int> dl, ll;
+  for (int b = 0; b < p->nb * p->nb; ++b) {
+    if (p->dslot_h[b] >= 0) dl.push_back(b);
+    else ll.push_back(b);
+  }
+  int *d_dl = nullptr, *d_ll = nullptr;
+  CUDA_TRY(dalloc(&d_dl, dl.size()));
+  CUDA_TRY(dalloc(&d_ll, ll.size()));
+  if (!dl.empty()) CUDA_TRY(cudaMemcpy(d_dl, dl.data(), sizeof(int) * dl.size(), cudaMemcpyHostToDevice));
+  if (!ll.empty()) CUDA_TRY(cudaMemcpy(d_ll, ll.data(), sizeof(int) * ll.size(), cudaMemcpyHostToDevice));
+  BlrView<double> H = h_view(p);
+  if (!dl.empty()) k_build_dense<<<(int)std::min<size_t>(dl.size(), 4096), 256, 0, s>>>(H, K, d_dl, (int)dl.size());
+  int rc = FRANK_OK;
+  if (!ll.empty()) {
+    const int64_t bm = p->bmax;
+    const int64_t stride = 3 * bm * bm + 6 * bm;
+    const int grid = (int)std::min<size_t>(ll.size(), (size_t)2 * p->sm_count);
+    double* scratch = nullptr;
+    CUDA_TRY(cudaMalloc(&scratch, sizeof(double) * stride * grid));
+    CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
+    k_build_lowrank<<<grid, BUILD_THREADS, 0, s>>>(H, K, d_ll, (int)ll.size(), eps, scratch, stride, p->err);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaMemcpy(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(scratch);
+    if (p->err_h[ERR_RANK_OVERFLOW]) rc = fail(FRANK_ERR_RANK_OVERFLOW, "a compressed block exceeded max_rank and was truncated");
+  }
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(dx);
+  if (d_dl) cudaFree(d_dl);
+  if (d_ll) cudaFree(d_ll);
+  p->factored = false;
+  return rc;
+}
+
+int frank_blr_block_info(const frank_blr* p, int which, int i, int j, int* type, int* rank) {
+  int rc = check_block(p, i, j);
+  if (rc) return rc;
+  const bool lr = p->lslot_h[i * p->nb + j] >= 0;
+  if (type) *type = lr ? FRANK_BLOCK_LOWRANK : FRANK_BLOCK_DENSE;
+  if (rank) {
+    *rank = 0;
+    if (lr) CUDA_TRY(cudaMemcpy(rank, (which ? p->d_rankW : p->d_rankH) + i * p->nb + j, sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  return FRANK_OK;
+}
+
+
+int frank_blr_get_dense(const frank_blr* p, int which, int i, int j, double* a, int64_t ld, int rowmajor) {
+  int rc = check_block(p, i, j);
+  if (rc) return rc;
+  const int s = p->dslot_h[i * p->nb + j];
+  if (s < 0) return fail(FRANK_ERR_INVALID, "block is low rank");
+  const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j];
+  const size_t cnt = (size_t)p->bmax * p->bmax;
+  const char* base = which ? static_cast<const char*>(p->Wd) + s * cnt * tsize(p)
+                           : reinterpret_cast<const char*>(p->Hd + s * cnt);
+  std::vector<double> h;
+  if ((rc = fetch(p, which, base, cnt, h))) return rc;
+  for (int c = 0; c < bj; ++c)
+    for (int r = 0; r < bi; ++r) {
+      const double v = h[r + (size_t)c * p->bmax];
+      if (rowmajor) a[(size_t)r * ld + c] = v; else a[r + (size_t)c * ld] = v;
+    }
+  return FRANK_OK;
+}
+
+int frank_blr_get_lowrank(const frank_blr* p, int which, int i, int j, double* U, int64_t ldu, double* S,
+                          int64_t lds, double* V, int64_t ldv, int rowmajor) {
+  int rc = check_block(p, i, j);
+  if (rc) return rc;
+  const int s = p->lslot_h[i * p->nb + j];
+  if (s < 0) return fail(FRANK_ERR_INVALID, "block is dense");
+  int rank = 0;
+  CUDA_TRY(cudaMemcpy(&rank, (which ? p->d_rankW : p->d_rankH) + i * p->nb + j, sizeof(int), cudaMemcpyDeviceToHost));
+  const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j];
+  const size_t bm = p->bmax, kc = p->kcap;
+  const size_t es = which ? tsize(p) : sizeof(double);
+  const char* bu = which ? static_cast<const char*>(p->Wu) : reinterpret_cast<const char*>(p->Hu);
+  const char* bs = which ? static_cast<const char*>(p->Ws) : reinterpret_cast<const char*>(p->Hs);
+  const char* bv = which ? static_cast<const char*>(p->Wv) : reinterpret_cast<const char*>(p->Hv);
+  std::vector<double> hu, hs, hv;
+  if ((rc = fetch(p, which, bu + s * bm * kc * es, bm * kc, hu))) return rc;
+  if ((rc = fetch(p, which, bs + s * kc * kc * es, kc * kc, hs))) return rc;
+  if ((rc = fetch(p, which, bv + s * bm * kc * es, bm * kc, hv))) return rc;
+  for (int c = 0; c < rank; ++c)
+    for (int r = 0; r < bi; ++r) {
+      const double v = hu[r + c * bm];
+      if (rowmajor) U[(size_t)r * ldu + c] = v; else U[r + (size_t)c * ldu] = v;
+    }
+  for (int c = 0; c < rank; ++c)
+    for (int r = 0; r < rank; ++r) {
+      const double v = hs[r + c * kc];
+      if (rowmajor) S[(size_t)r * lds + c] = v; else S[r + (size_t)c * lds] = v;
+    }
+  for (int a = 0; a < rank; ++a)
+    for (int c = 0; c < bj; ++c) {
+      const double v = hv[c + a * bm];
+      if (rowmajor) V[(size_t)a * ldv + c] = v; else V[a + (size_t)c * ldv] = v;
+    }
+  return FRANK_OK;
+}
+
+int frank_blr_get_pivots(const frank_blr* p, int i, int* ipiv) {
+  int rc = check_block(p, i, i);
+  if (rc) return rc;
+  if (!p->factored) return fail(FRANK_ERR_STATE, "pivots before getrf");
+  const int b = p->off_h[i + 1] - p->off_h[i];
+  CUDA_TRY(cudaMemcpy(ipiv, p->ipiv + (size_t)i * p->bmax, sizeof(int) * b, cudaMemcpyDeviceToHost));
+  for (int r = 0; r < b; ++r) ipiv[r] += 1;
+  return FRANK_OK;
+}
+
+int frank_blr_getrf(frank_blr* p, void* stream) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!s) {
+    if (!p->graph_stream) CUDA_TRY(cudaStreamCreateWithFlags(&p->graph_stream, cudaStreamNonBlocking));
+    s = p->graph_stream;
+  }
+  p->factored = false;
+  return p->precision == FRANK_PREC_FP64 ? run_factor<double>(p, s) : run_factor<float>(p, s);
+}
+
+int frank_blr_solve_device(frank_blr* p, double* d_b, int64_t ldb, int nrhs, void* stream) {
+  if (!p || !d_b || nrhs < 1 || ldb < p->n) return fail(FRANK_ERR_INVALID, "bad solve arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = solve_device_impl(p, d_b, ldb, nrhs, false, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return FRANK_OK;
+}
+
+int frank_blr_solve_transpose_device(frank_blr* p, double* d_b, int64_t ldb, int nrhs, void* stream) {
+  if (!p || !d_b || nrhs < 1 || ldb < p->n) return fail(FRANK_ERR_INVALID, "bad solve arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = solve_device_impl(p, d_b, ldb, nrhs, true, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return FRANK_OK;
+}
+
+int frank_blr_solve(frank_blr* p, double* b, int64_t ldb, int nrhs, void* stream) {
+  if (!p || !b || nrhs < 1 || ldb < p->n) return fail(FRANK_ERR_INVALID, "bad solve arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, sizeof(double) * p->n * nrhs));
+  CUDA_TRY(cudaMemcpy2DAsync(d, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyHostToDevice, s));
+  int rc = solve_device_impl(p, d, p->n, nrhs, false, s);
+  if (rc == FRANK_OK) {
+    cudaError_t e = cudaMemcpy2DAsync(b, ldb * sizeof(double), d, p->n * sizeof(double), p->n * sizeof(double), nrhs,
+                                      cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaFree(d);
+  return rc;
+}
+
+int frank_blr_matvec_device(frank_blr* p, const double* d_x, int64_t ldx, double* d_y, int64_t ldy, int nrhs,
+                            void* stream) {
+  if (!p || !d_x || !d_y || nrhs < 1 || ldx < p->n || ldy < p->n) return fail(FRANK_ERR_INVALID, "bad matvec arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = matvec_device_impl(p, d_x, ldx, d_y, ldy, nrhs, nullptr, 0, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return FRANK_OK;
+}
+
+int frank_blr_matvec(frank_blr* p, const double* x, int64_t ldx, double* y, int64_t ldy, int nrhs, void* stream) {
+  if (!p || !x || !y || nrhs < 1 || ldx < p->n || ldy < p->n) return fail(FRANK_ERR_INVALID, "bad matvec arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *dx = nullptr, *dy = nullptr;
+  CUDA_TRY(cudaMalloc(&dx, sizeof(double) * p->n * nrhs));
+  CUDA_TRY(cudaMalloc(&dy, sizeof(double) * p->n * nrhs));
+  CUDA_TRY(cudaMemcpy2DAsync(dx, p->n * sizeof(double), x, ldx * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyHostToDevice, s));
+  int rc = matvec_device_impl(p, dx, p->n, dy, p->n, nrhs, nullptr, 0, s);
+  if (rc == FRANK_OK) {
+    cudaError_t e = cudaMemcpy2DAsync(y, ldy * sizeof(double), dy, p->n * sizeof(double), p->n * sizeof(double), nrhs,
+                                      cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaFree(dx);
+  cudaFree(dy);
+  return rc;
+}
+
+int frank_blr_refine_device(frank_blr* p, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int nrhs,
+                            double tol, int maxit, int* iters, double* resid, void* stream) {
+  if (!p || !d_b || !d_x || nrhs < 1 || ldb < p->n || ldx < p->n || maxit < 0)
+    return fail(FRANK_ERR_INVALID, "bad refine arguments");
+  return refine_device_impl(p, d_b, ldb, d_x, ldx, nrhs, tol, maxit, iters, resid, static_cast<cudaStream_t>(stream));
+}
+
+int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int64_t ldx, int nrhs, double tol,
+                     int maxit, int* iters, double* resid, void* stream) {
+  if (!p || !b || !x || nrhs < 1 || ldb < p->n || ldx < p->n || maxit < 0)
+    return fail(FRANK_ERR_INVALID, "bad refine arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *db = nullptr, *dx = nullptr;
+  CUDA_TRY(cudaMalloc(&db, sizeof(double) * p->n * nrhs));
+  CUDA_TRY(cudaMalloc(&dx, sizeof(double) * p->n * nrhs));
+  CUDA_TRY(cudaMemcpy2DAsync(db, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyHostToDevice, s));
+  int rc = refine_device_impl(p, db, p->n, dx, p->n, nrhs, tol, maxit, iters, resid, s);
+  if (rc == FRANK_OK || rc == FRANK_ERR_NOT_CONVERGED) {
+    cudaError_t e = cudaMemcpy2DAsync(x, ldx * sizeof(double), dx, p->n * sizeof(double), p->n * sizeof(double), nrhs,
+                                      cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaFree(db);
+  cudaFree(dx);
+  return rc;
+}
+
+int frank_blr_stats(const frank_blr* p, int64_t* launches, int64_t* recompressions, int64_t* max_rank_seen,
+                    int64_t* rank_overflows) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  if (launches) *launches = p->launches;
+  if (recompressions) *recompressions = p->err_h[ERR_RECOMP];
+  if (max_rank_seen) *max_rank_seen = p->err_h[ERR_MAX_RANK];
+  if (rank_overflows) *rank_overflows = p->err_h[ERR_RANK_OVERFLOW];
+  return FRANK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1101 @@
+// Kernels of the BLR-LU factor-and-solve path (sm_100a).
+//
+// Storage (all column-major):
+//   * dense block (i,j): bmax x bmax slot, ld = bmax, of which bs(i) x bs(j) used;
+//   * low-rank block (i,j) = U S V: U (bmax x kcap, ld bmax), S (kcap x kcap,
+//     ld kcap), Vt = V^T (bmax x kcap, ld bmax); rank r = rank[i*nb+j] columns used.
+// T is the working precision (double for the plain FP64 path, float for the
+// mixed path); every small factorization (leaf getrf, stacked-basis QR, core
+// SVD) is computed in FP64.
+#pragma once
+
+#include "common.cuh"
+
+namespace frank {
+
+template <typename T>
+struct BlrView {
+  int nb, bmax, kcap;
+  const int* off;    // [nb+1] block offsets
+  const int* dslot;  // [nb*nb] dense slot or -1
+  const int* lslot;  // [nb*nb] low-rank slot or -1
+  int* rank;         // [nb*nb] current ranks (low-rank blocks)
+  T* D;
+  T* U;
+  T* S;
+  T* Vt;
+  FRANK_D int bs(int i) const { return off[i + 1] - off[i]; }
+  FRANK_D bool is_lr(int i, int j) const { return lslot[i * nb + j] >= 0; }
+  FRANK_D T* dense(int i, int j) const { return D + (int64_t)dslot[i * nb + j] * bmax * bmax; }
+  FRANK_D T* u(int i, int j) const { return U + (int64_t)lslot[i * nb + j] * bmax * kcap; }
+  FRANK_D T* s(int i, int j) const { return S + (int64_t)lslot[i * nb + j] * kcap * kcap; }
+  FRANK_D T* vt(int i, int j) const { return Vt + (int64_t)lslot[i * nb + j] * bmax * kcap; }
+};
+
+// Per-factorization workspace (device pointers).
+template <typename T>
+struct FactorWs {
+  int* perm;      // [nb][bmax]: row i of P*B is row perm[i] of B, per diagonal block
+  int* ipiv;      // [nb][bmax]: LAPACK-style 0-based pivots per diagonal block
+  T* Linv;        // [nb][bmax*bmax]: unit-lower inverse per diagonal block
+  T* Uinv;        // [nb][bmax*bmax]: upper inverse per diagonal block
+  T* WL;          // [nb][bmax*bmax]: (S V)^T of column-panel blocks, by block row
+  T* WU;          // [nb][bmax*bmax]: U S of row-panel blocks, by block column
+  double* getrf_scratch;  // bmax*bmax
+  double* dscratch;       // dense-update scratch, per CTA slot
+  int64_t dscratch_stride;
+  double* rscratch;       // recompression scratch, per CTA slot
+  int64_t rscratch_stride;
+  int* err;
+  int fixed_rank;
+  double eps;
+};
+
+// ---------------------------------------------------------------------------
+// Reset the working copy from A_H (FP64) -- only the used parts are copied.
+// One CTA per block.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_reset(BlrView<double> H, BlrView<T> W) {
+  const int blk = blockIdx.x;
+  const int i = blk / H.nb, j = blk % H.nb;
+  const int bi = H.bs(i), bj = H.bs(j);
+  if (H.lslot[blk] >= 0) {
+    const int r = H.rank[blk];
+    const double* hu = H.u(i, j); const double* hs = H.s(i, j); const double* hv = H.vt(i, j);
+    T* wu = W.u(i, j); T* ws = W.s(i, j); T* wv = W.vt(i, j);
+    for (int64_t e = threadIdx.x; e < (int64_t)bi * r; e += blockDim.x) {
+      const int rr = e % bi, c = e / bi;
+      wu[rr + (int64_t)c * W.bmax] = T(hu[rr + (int64_t)c * H.bmax]);
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)bj * r; e += blockDim.x) {
+      const int rr = e % bj, c = e / bj;
+      wv[rr + (int64_t)c * W.bmax] = T(hv[rr + (int64_t)c * H.bmax]);
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
+      const int rr = e % r, c = e / r;
+      ws[rr + (int64_t)c * W.kcap] = T(hs[rr + (int64_t)c * H.kcap]);
+    }
+    if (threadIdx.x == 0) W.rank[blk] = r;
+  } else if (H.dslot[blk] >= 0) {
+    const double* hd = H.dense(i, j);
+    T* wd = W.dense(i, j);
+    for (int64_t e = threadIdx.x; e < (int64_t)bi * bj; e += blockDim.x) {
+      const int rr = e % bi, c = e / bi;
+      wd[rr + (int64_t)c * W.bmax] = T(hd[rr + (int64_t)c * H.bmax]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K1: leaf getrf of diagonal block i with partial pivoting, FP64, one CTA
+// (512 threads).  Blocked right-looking LU (panel width 32): the panel is
+// factored column by column (idamax pivot, row swap across the whole block,
+// reciprocal scaling and rank-1 update as in LAPACK dgetf2), then the row
+// block is solved with the unit-lower 32x32 triangle and the trailing matrix
+// updated by a CTA GEMM.  Then the explicit inverses of the unit-lower L and
+// the upper U are formed by blocked triangular inversion (LAPACK dtrtri
+// column-block order).  Writes the packed LU back into the block, the
+// pivots/permutation, Linv and Uinv in T.
+// ---------------------------------------------------------------------------
+constexpr int GETRF_THREADS = 512;
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<T> ws, int i) {
+  __shared__ double red[32];
+  __shared__ int redi[32];
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ double tri[32 * 33];
+  const int b = A.bs(i);
+  const int ldA = A.bmax;
+  T* Dp = A.dense(i, i);
+  double* Wm = ws.getrf_scratch;
+  int* piv = ws.ipiv + (int64_t)i * A.bmax;
+  int* perm = ws.perm + (int64_t)i * A.bmax;
+  T* Li = ws.Linv + (int64_t)i * A.bmax * A.bmax;
+  T* Ui = ws.Uinv + (int64_t)i * A.bmax * A.bmax;
+  for (int64_t e = threadIdx.x; e < (int64_t)b * b; e += blockDim.x) {
+    const int r = e % b, c = e / b;
+    Wm[r + (int64_t)c * b] = double(Dp[r + (int64_t)c * ldA]);
+  }
+  __syncthreads();
+  int first_zero = -1;
+  for (int jb = 0; jb < b; jb += 32) {
+    const int jn = min(32, b - jb);
+    for (int j = jb; j < jb + jn; ++j) {
+      double best = -1.0;
+      int bi = -1;
+      for (int r = j + threadIdx.x; r < b; r += blockDim.x) {
+        const double a = fabs(Wm[r + (int64_t)j * b]);
+        if (a > best) { best = a; bi = r; }
+      }
+      double amax;
+      const int p = block_argmax_abs(best < 0.0 ? 0.0 : best, bi, red, redi, &amax);
+      if (threadIdx.x == 0) piv[j] = p;
+      if (amax == 0.0 && first_zero < 0) first_zero = j;
+      if (p != j && amax != 0.0) {
+        for (int c = threadIdx.x; c < b; c += blockDim.x) {
+          const double t = Wm[j + (int64_t)c * b];
+          Wm[j + (int64_t)c * b] = Wm[p + (int64_t)c * b];
+          Wm[p + (int64_t)c * b] = t;
+        }
+      }
+      __syncthreads();
+      if (amax != 0.0) {
+        const double rcp = 1.0 / Wm[j + (int64_t)j * b];
+        for (int r = j + 1 + threadIdx.x; r < b; r += blockDim.x) Wm[r + (int64_t)j * b] *= rcp;
+      }
+      __syncthreads();
+      const int nr = b - j - 1, nc = jb + jn - j - 1;
+      for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+        const int r = j + 1 + e % nr, c = j + 1 + e / nr;
+        Wm[r + (int64_t)c * b] -= Wm[r + (int64_t)j * b] * Wm[j + (int64_t)c * b];
+      }
+      __syncthreads();
+    }
+    // U12 = L11^{-1} A12
+    for (int c = jb + jn + threadIdx.x; c < b; c += blockDim.x) {
+      for (int r = 1; r < jn; ++r) {
+        double s = Wm[(jb + r) + (int64_t)c * b];
+        for (int t = 0; t < r; ++t) s -= Wm[(jb + r) + (int64_t)(jb + t) * b] * Wm[(jb + t) + (int64_t)c * b];
+        Wm[(jb + r) + (int64_t)c * b] = s;
+      }
+    }
+    __syncthreads();
+    const int m2 = b - jb - jn;
+    if (m2 > 0)
+      cta_gemm<double, GETRF_THREADS>(m2, m2, jn, -1.0, Wm + (jb + jn) + (int64_t)jb * b, b, false,
+                                      Wm + jb + (int64_t)(jb + jn) * b, b, false, 1.0,
+                                      Wm + (jb + jn) + (int64_t)(jb + jn) * b, b, gsm);
+  }
+  if (threadIdx.x == 0) {
+    if (first_zero >= 0) atomicCAS(ws.err + ERR_SINGULAR_STEP, 0, i + 1);
+    // permutation from the interchanges: (P B)[r] = B[perm[r]]
+    for (int r = 0; r < b; ++r) perm[r] = r;
+    for (int r = 0; r < b; ++r) {
+      const int p = piv[r];
+      const int t = perm[r]; perm[r] = perm[p]; perm[p] = t;
+    }
+  }
+  // packed LU back into the block
+  for (int64_t e = threadIdx.x; e < (int64_t)b * b; e += blockDim.x) {
+    const int r = e % b, c = e / b;
+    Dp[r + (int64_t)c * ldA] = T(Wm[r + (int64_t)c * b]);
+  }
+  __syncthreads();
+  // ---- Uinv: X = U^{-1}, blocked by 32-column blocks from the left ----
+  // X[0:j, j:j+jn] = -(X[0:j,0:j] U[0:j, j:j+jn]) inv(U_jj); X_jj = inv(U_jj).
+  // Built in FP64 in the Linv/Uinv slot of T is not possible for T=float, so
+  // the FP64 result is staged in the upper triangle region of a second FP64
+  // buffer: we reuse Wm's strictly-lower part? No -- keep it simple: compute
+  // each output block column into shared memory and write it in T, reading
+  // previously written columns back from T (ok: values are rounded once).
+  for (int jb = 0; jb < b; jb += 32) {
+    const int jn = min(32, b - jb);
+    // inv(U_jj) into tri (jn x jn, ld 33)
+    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
+    __syncthreads();
+    if (threadIdx.x < jn) {
+      const int c = threadIdx.x;
+      tri[c + c * 33] = 1.0 / Wm[(jb + c) + (int64_t)(jb + c) * b];
+      for (int r = c - 1; r >= 0; --r) {
+        double s = 0.0;
+        for (int t = r + 1; t <= c; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
+        tri[r + c * 33] = -s / Wm[(jb + r) + (int64_t)(jb + r) * b];
+      }
+    }
+    __syncthreads();
+    // zero the column block of Ui, write the diagonal block
+    for (int e = threadIdx.x; e < b * jn; e += blockDim.x) {
+      const int r = e % b, c = e / b;
+      double v = 0.0;
+      if (r >= jb && r < jb + jn) v = tri[(r - jb) + c * 33];
+      Ui[r + (int64_t)(jb + c) * ldA] = T(v);
+    }
+    __syncthreads();
+    if (jb > 0) {
+      // tmp (jb x jn) = X[0:jb, 0:jb] * U[0:jb, jb:jb+jn]  -> stored in Wm's
+      // strictly-lower area is unsafe; use the Li slot as FP64-free temp is
+      // also T-typed.  So compute column by column with FP64 registers:
+      // each thread owns (row r, col c) and accumulates over t in [r, jb).
+      for (int e = threadIdx.x; e < jb * jn; e += blockDim.x) {
+        const int r = e % jb, c = e / jb;
+        double s = 0.0;
+        for (int t = r; t < jb; ++t) s += double(Ui[r + (int64_t)t * ldA]) * Wm[t + (int64_t)(jb + c) * b];
+        // multiply by inv(U_jj) later: stash s in Li (T) temporarily
+        Li[r + (int64_t)c * ldA] = T(s);
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < jb * jn; e += blockDim.x) {
+        const int r = e % jb, c = e / jb;
+        double s = 0.0;
+        for (int t = 0; t <= c; ++t) s += double(Li[r + (int64_t)t * ldA]) * tri[t + c * 33];
+        Ui[r + (int64_t)(jb + c) * ldA] = T(-s);
+      }
+      __syncthreads();
+    }
+  }
+  // ---- Linv: X = L^{-1} (unit lower), blocked from the bottom ----
+  // X[j+jn:b, j:j+jn] = -(X[j+jn:b, j+jn:b] L[j+jn:b, j:j+jn]) inv(L_jj)
+  const int nblk = (b + 31) / 32;
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int jb = blk * 32;
+    const int jn = min(32, b - jb);
+    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
+    __syncthreads();
+    if (threadIdx.x < jn) {
+      const int c = threadIdx.x;
+      tri[c + c * 33] = 1.0;
+      for (int r = c + 1; r < jn; ++r) {
+        double s = 0.0;
+        for (int t = c; t < r; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
+        tri[r + c * 33] = -s;
+      }
+    }
+    __syncthreads();
+    const int below = b - jb - jn;
+    // temp product into the (not yet written) upper rows [0, jb) of this
+    // column block of Li, which are zero in the final result
+    if (below > 0) {
+      // product P (below x jn) = X[jb+jn:, jb+jn:] * L[jb+jn:, jb:jb+jn]
+      // stash in FP64 inside Wm's upper triangle is not allowed (U still
+      // needed? no: U is already in Dp and Ui), so use Wm's upper-right part.
+      double* tmp = Wm;  // overwrite rows 0..below-1, cols 0..jn-1 of Wm (U part no longer needed except L below)
+      // Wm's upper triangle (r < c) held U; U is consumed.  Rows 0..below-1 x
+      // cols 0..jn-1 overlap the lower part when r > c, so use a column
+      // offset that keeps us strictly in the upper triangle: cols [b-jn, b)
+      // with rows [0, below): r < below <= b - jn <= c  => r < c.  Safe.
+      for (int e = threadIdx.x; e < below * jn; e += blockDim.x) {
+        const int r = e % below, c = e / below;
+        double s = 0.0;
+        const int gr = jb + jn + r;
+        for (int t = jb + jn; t <= gr; ++t) s += double(Li[gr + (int64_t)t * ldA]) * Wm[t + (int64_t)(jb + c) * b];
+        tmp[r + (int64_t)(b - jn + c) * b] = s;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < below * jn; e += blockDim.x) {
+        const int r = e % below, c = e / below;
+        double s = 0.0;
+        for (int t = c; t < jn; ++t) s += tmp[r + (int64_t)(b - jn + t) * b] * tri[t + c * 33];
+        Li[(jb + jn + r) + (int64_t)(jb + c) * ldA] = T(-s);
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < (jb + jn) * jn; e += blockDim.x) {
+      const int r = e % (jb + jn), c = e / (jb + jn);
+      double v = 0.0;
+      if (r >= jb) v = tri[(r - jb) + c * 33];
+      Li[r + (int64_t)(jb + c) * ldA] = T(v);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: panel of step i.  Task t < m: column-panel block (i+1+t, i):
+//   low rank: V <- V Uinv (Vt <- Uinv^T Vt), then WL = Vt S^T;
+//   dense:    A <- A Uinv.
+// Task t >= m: row-panel block (i, i+1+t-m):
+//   low rank: U <- Linv P U, then WU = U S;   dense: A <- Linv P A.
+// (trsm.cpp:92-115 with the leaf inverse; the pivots of K1 applied.)
+// ---------------------------------------------------------------------------
+constexpr int PANEL_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel(BlrView<T> A, FactorWs<T> ws, int i) {
+  __shared__ T gsm[2 * 16 * 64];
+  const int m = A.nb - i - 1;
+  const int t = blockIdx.x;
+  const int bi = A.bs(i);
+  const int ld = A.bmax;
+  const T* Li = ws.Linv + (int64_t)i * ld * ld;
+  const T* Ui = ws.Uinv + (int64_t)i * ld * ld;
+  const int* perm = ws.perm + (int64_t)i * ld;
+  if (t < m) {
+    const int ic = i + 1 + t;
+    T* tmp = ws.WL + (int64_t)ic * ld * ld;
+    if (A.is_lr(ic, i)) {
+      const int r = A.rank[ic * A.nb + i];
+      T* vt = A.vt(ic, i);
+      // tmp = Uinv^T * Vt   (bi x r)
+      cta_gemm<T, PANEL_THREADS>(bi, r, bi, T(1), Ui, ld, true, vt, ld, false, T(0), tmp, ld, gsm);
+      for (int64_t e = threadIdx.x; e < (int64_t)bi * r; e += blockDim.x) {
+        const int rr = e % bi, c = e / bi;
+        vt[rr + (int64_t)c * ld] = tmp[rr + (int64_t)c * ld];
+      }
+      __syncthreads();
+      // WL = Vt * S^T
+      cta_gemm<T, PANEL_THREADS>(bi, r, r, T(1), vt, ld, false, A.s(ic, i), A.kcap, true, T(0), tmp, ld, gsm);
+    } else {
+      const int bc = A.bs(ic);
+      T* a = A.dense(ic, i);
+      // tmp = A * Uinv  (bc x bi), then copy back
+      cta_gemm<T, PANEL_THREADS>(bc, bi, bi, T(1), a, ld, false, Ui, ld, false, T(0), tmp, ld, gsm);
+      for (int64_t e = threadIdx.x; e < (int64_t)bc * bi; e += blockDim.x) {
+        const int rr = e % bc, c = e / bc;
+        a[rr + (int64_t)c * ld] = tmp[rr + (int64_t)c * ld];
+      }
+    }
+  } else {
+    const int k = i + 1 + (t - m);
+    T* tmp = ws.WU + (int64_t)k * ld * ld;
+    if (A.is_lr(i, k)) {
+      const int r = A.rank[i * A.nb + k];
+      T* u = A.u(i, k);
+      for (int64_t e = threadIdx.x; e < (int64_t)bi * r; e += blockDim.x) {
+        const int rr = e % bi, c = e / bi;
+        tmp[rr + (int64_t)c * ld] = u[perm[rr] + (int64_t)c * ld];
+      }
+      __syncthreads();
+      cta_gemm<T, PANEL_THREADS>(bi, r, bi, T(1), Li, ld, false, tmp, ld, false, T(0), u, ld, gsm);
+      // WU = U * S
+      cta_gemm<T, PANEL_THREADS>(bi, r, r, T(1), u, ld, false, A.s(i, k), A.kcap, false, T(0), tmp, ld, gsm);
+    } else {
+      const int bk = A.bs(k);
+      T* a = A.dense(i, k);
+      for (int64_t e = threadIdx.x; e < (int64_t)bi * bk; e += blockDim.x) {
+        const int rr = e % bi, c = e / bi;
+        tmp[rr + (int64_t)c * ld] = a[perm[rr] + (int64_t)c * ld];
+      }
+      __syncthreads();
+      cta_gemm<T, PANEL_THREADS>(bi, bk, bi, T(1), Li, ld, false, tmp, ld, false, T(0), a, ld, gsm);
+    }
+  }
+}
+
+// Operands of the update of target (ic, k) at step i:
+//   update = - XL * (WL^T WU) * YR^T,
+// XL = U(ic,i) (bc x p) or dense A(ic,i) (bc x bi, WL = I),
+// YR = Vt(i,k) (bk x q) or A(i,k)^T (WU = I).
+template <typename T>
+struct UpdOps {
+  const T* XL; int p; bool left_dense;
+  const T* YR; int q; bool right_dense;   // right_dense: YR^T = A(i,k) (bi x bk, ld)
+  const T* WL; const T* WU;
+};
+
+template <typename T>
+FRANK_D UpdOps<T> update_operands(const BlrView<T>& A, const FactorWs<T>& ws, int i, int ic, int k) {
+  UpdOps<T> o;
+  const int ld = A.bmax;
+  const int bi = A.bs(i);
+  o.WL = ws.WL + (int64_t)ic * ld * ld;
+  o.WU = ws.WU + (int64_t)k * ld * ld;
+  if (A.is_lr(ic, i)) { o.XL = A.u(ic, i); o.p = A.rank[ic * A.nb + i]; o.left_dense = false; }
+  else { o.XL = A.dense(ic, i); o.p = bi; o.left_dense = true; }
+  if (A.is_lr(i, k)) { o.YR = A.vt(i, k); o.q = A.rank[i * A.nb + k]; o.right_dense = false; }
+  else { o.YR = A.dense(i, k); o.q = bi; o.right_dense = true; }
+  return o;
+}
+
+// core T (p x q) = -WL^T WU, FP64, into Tm (ld p).
+template <typename T, int NT>
+FRANK_D void form_core(const UpdOps<T>& o, int bi, int ld, double* Tm, double* gsm) {
+  if (!o.left_dense && !o.right_dense) {
+    cta_gemm<double, NT>(o.p, o.q, bi, -1.0, o.WL, ld, true, o.WU, ld, false, 0.0, Tm, o.p, gsm);
+  } else if (!o.left_dense && o.right_dense) {
+    // -WL^T (p x bi)
+    for (int64_t e = threadIdx.x; e < (int64_t)o.p * o.q; e += blockDim.x) {
+      const int r = e % o.p, c = e / o.p;
+      Tm[e] = -double(o.WL[c + (int64_t)r * ld]);
+    }
+    __syncthreads();
+  } else if (o.left_dense && !o.right_dense) {
+    for (int64_t e = threadIdx.x; e < (int64_t)o.p * o.q; e += blockDim.x) {
+      const int r = e % o.p, c = e / o.p;
+      Tm[e] = -double(o.WU[r + (int64_t)c * ld]);
+    }
+    __syncthreads();
+  } else {
+    for (int64_t e = threadIdx.x; e < (int64_t)o.p * o.q; e += blockDim.x) {
+      const int r = e % o.p, c = e / o.p;
+      Tm[e] = (r == c) ? -1.0 : 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5: update of dense targets (diagonal blocks and inadmissible blocks):
+// C += XL * T * YR^T  (gemm.cpp:180-200 for LR.LR.D; 126-178 for the others).
+// Persistent grid over the m*m targets of the step, skipping low-rank ones.
+// ---------------------------------------------------------------------------
+constexpr int DUPD_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i) {
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ T gsmt[2 * 16 * 64];
+  const int m = A.nb - i - 1;
+  const int ld = A.bmax;
+  const int bi = A.bs(i);
+  double* Tm = ws.dscratch + (int64_t)blockIdx.x * ws.dscratch_stride;
+  T* X = reinterpret_cast<T*>(Tm + (int64_t)ld * ld);
+  for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
+    const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
+    if (A.is_lr(ic, k)) continue;
+    const int bc = A.bs(ic), bk = A.bs(k);
+    T* C = A.dense(ic, k);
+    UpdOps<T> o = update_operands(A, ws, i, ic, k);
+    if (o.left_dense && o.right_dense) {
+      // C -= A(ic,i) A(i,k)
+      cta_gemm<T, DUPD_THREADS>(bc, bk, bi, T(-1), o.XL, ld, false, o.YR, ld, false, T(1), C, ld, gsmt);
+      continue;
+    }
+    form_core<T, DUPD_THREADS>(o, bi, ld, Tm, gsm);
+    // X = XL * T  (bc x q), accumulate in the working precision
+    cta_gemm<T, DUPD_THREADS>(bc, o.q, o.p, T(1), o.XL, ld, false, Tm, o.p, false, T(0), X, ld, gsmt);
+    // C += X * YR^T
+    if (!o.right_dense)
+      cta_gemm<T, DUPD_THREADS>(bc, bk, o.q, T(1), X, ld, false, o.YR, ld, true, T(1), C, ld, gsmt);
+    else
+      cta_gemm<T, DUPD_THREADS>(bc, bk, o.q, T(1), X, ld, false, o.YR, ld, false, T(1), C, ld, gsmt);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K4: rounded addition of the update into every low-rank target of the step
+// (operations/arithmetic/addition.cpp:93-127, Bebendorf p.16):
+//   C + W = [U_C | XL] blockdiag(S_C, T) [Vt_C | YR]^T,
+//   QR of the stacked U bases and of the stacked V bases (Householder, FP64),
+//   core M = Ru blockdiag(S_C, T) Rv^T, one-sided Jacobi SVD of M (FP64),
+//   rank by find_svd_truncation_rank (misc.cpp:133-146, quirk included) or
+//   the fixed rank, new U = Qu Um_r, V^T = Qv Vm_r, S = Sigma_r.
+// Persistent grid; each CTA owns one scratch slot (FP64) of
+// rscratch_stride doubles.
+// ---------------------------------------------------------------------------
+constexpr int RECOMP_THREADS = 512;
+
+struct RecompLayout {
+  int64_t ash, bsh, tm, mtmp, mm, m0, sig, ord, xo, yo, tau_u, tau_v, total;
+};
+
+FRANK_HD RecompLayout recomp_layout(int bmax, int smax) {
+  // smax: max stacked width (kcap + max(p, q))
+  RecompLayout L;
+  int64_t o = 0;
+  auto take = [&](int64_t n) { int64_t r = o; o += (n + 31) & ~int64_t(31); return r; };
+  const int mu = smax < bmax ? smax : bmax;
+  L.ash = take((int64_t)bmax * smax);
+  L.bsh = take((int64_t)bmax * smax);
+  L.tm = take((int64_t)bmax * bmax);
+  L.mtmp = take((int64_t)mu * smax);
+  L.mm = take((int64_t)mu * mu);
+  L.m0 = take((int64_t)mu * mu);
+  L.sig = take(mu);
+  L.ord = take(mu);
+  L.xo = take((int64_t)bmax * mu);
+  L.yo = take((int64_t)bmax * mu);
+  L.tau_u = take(smax);
+  L.tau_v = take(smax);
+  L.total = o;
+  return L;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax) {
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ double red[32];
+  __shared__ int flag;
+  __shared__ int s_rank;
+  const int m = A.nb - i - 1;
+  const int ld = A.bmax;
+  const int bi = A.bs(i);
+  const RecompLayout L = recomp_layout(A.bmax, smax);
+  double* base = ws.rscratch + (int64_t)blockIdx.x * ws.rscratch_stride;
+  double* Ash = base + L.ash;
+  double* Bsh = base + L.bsh;
+  double* Tm = base + L.tm;
+  double* Mtmp = base + L.mtmp;
+  double* Mm = base + L.mm;
+  double* M0 = base + L.m0;
+  double* sig = base + L.sig;
+  int* ord = reinterpret_cast<int*>(base + L.ord);
+  double* Xo = base + L.xo;
+  double* Yo = base + L.yo;
+  double* tau_u = base + L.tau_u;
+  double* tau_v = base + L.tau_v;
+  for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
+    const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
+    if (!A.is_lr(ic, k)) continue;
+    const int blk = ic * A.nb + k;
+    const int bc = A.bs(ic), bk = A.bs(k);
+    const int kc = A.rank[blk];
+    UpdOps<T> o = update_operands(A, ws, i, ic, k);
+    const int su = kc + o.p, sv = kc + o.q;
+    if (su > smax || sv > smax) {
+      if (threadIdx.x == 0) atomicAdd(ws.err + ERR_BOUNDS, 1);
+      continue;
+    }
+    T* Uc = A.u(ic, k);
+    T* Sc = A.s(ic, k);
+    T* Vc = A.vt(ic, k);
+    // stacked bases in FP64
+    for (int64_t e = threadIdx.x; e < (int64_t)bc * su; e += blockDim.x) {
+      const int r = e % bc, c = e / bc;
+      double v;
+      if (c < kc) v = double(Uc[r + (int64_t)c * ld]);
+      else v = double(o.XL[r + (int64_t)(c - kc) * ld]);
+      Ash[r + (int64_t)c * bc] = v;
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)bk * sv; e += blockDim.x) {
+      const int r = e % bk, c = e / bk;
+      double v;
+      if (c < kc) v = double(Vc[r + (int64_t)c * ld]);
+      else if (!o.right_dense) v = double(o.YR[r + (int64_t)(c - kc) * ld]);
+      else v = double(o.YR[(c - kc) + (int64_t)r * ld]);  // A(i,k)^T
+      Bsh[r + (int64_t)c * bk] = v;
+    }
+    form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
+    cta_householder_qr(bc, su, Ash, bc, tau_u, red);
+    cta_householder_qr(bk, sv, Bsh, bk, tau_v, red);
+    const int mu = min(bc, su), mv = min(bk, sv);
+    // Mtmp (mu x sv) = Ru * blockdiag(S_C, T)
+    for (int64_t e = threadIdx.x; e < (int64_t)mu * sv; e += blockDim.x) {
+      const int r = e % mu, c = e / mu;
+      double s = 0.0;
+      if (c < kc) {
+        for (int t = r; t < kc; ++t) s += Ash[r + (int64_t)t * bc] * double(Sc[t + (int64_t)c * A.kcap]);
+      } else {
+        const int cc = c - kc;
+        for (int t = max(r, kc); t < su; ++t) s += Ash[r + (int64_t)t * bc] * Tm[(t - kc) + (int64_t)cc * o.p];
+      }
+      Mtmp[r + (int64_t)c * mu] = s;
+    }
+    __syncthreads();
+    // M (mu x mv) = Mtmp * Rv^T ; Rv (mv x sv) upper trapezoid in Bsh
+    for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) {
+      const int r = e % mu, c = e / mu;
+      double s = 0.0;
+      for (int t = c; t < sv; ++t) s += Mtmp[r + (int64_t)t * mu] * Bsh[c + (int64_t)t * bk];
+      Mm[r + (int64_t)c * mu] = s;
+      M0[r + (int64_t)c * mu] = s;
+    }
+    __syncthreads();
+    const int sweeps = cta_jacobi_columns(mu, mv, Mm, mu, 60, &flag);
+    if (sweeps < 0 && threadIdx.x == 0) atomicAdd(ws.err + ERR_JACOBI, 1);
+    // column norms
+    for (int c = threadIdx.x >> 5; c < mv; c += blockDim.x >> 5) {
+      double s = 0.0;
+      for (int r = threadIdx.x & 31; r < mu; r += 32) s += Mm[r + (int64_t)c * mu] * Mm[r + (int64_t)c * mu];
+      s = warp_sum(s);
+      if ((threadIdx.x & 31) == 0) sig[c] = sqrt(s);
+    }
+    __syncthreads();
+    // descending order: rank of each column = #(larger) + #(equal with smaller index)
+    for (int c = threadIdx.x; c < mv; c += blockDim.x) {
+      const double v = sig[c];
+      int pos = 0;
+      for (int d = 0; d < mv; ++d) {
+        const double w = sig[d];
+        pos += (w > v) || (w == v && d < c);
+      }
+      ord[pos] = c;
+    }
+    __syncthreads();
+    const int nsv = min(mu, mv);
+    if (threadIdx.x == 0) {
+      int r;
+      if (ws.fixed_rank > 0) {
+        r = min(ws.fixed_rank, nsv);
+      } else {
+        double fro = 0.0;
+        for (int j = 0; j < nsv; ++j) { const double v = sig[ord[j]]; fro += v * v; }
+        const double thr = ws.eps * sqrt(fro);
+        r = 0;
+        double err;
+        do {
+          ++r;
+          err = 0.0;
+          if (r < nsv) {
+            const double v = sig[ord[r]];
+            for (int j = r; j < nsv; ++j) err += v * v;
+          }
+        } while (r < nsv && sqrt(err) > thr);
+      }
+      if (r > A.kcap) { atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1); r = A.kcap; }
+      atomicMax(ws.err + ERR_MAX_RANK, r);
+      atomicAdd(ws.err + ERR_RECOMP, 1);
+      s_rank = r;
+    }
+    __syncthreads();
+    const int r = s_rank;
+    // Um_r (mu x r) normalized columns -> Xo (bc x r, rows >= mu zero)
+    for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+      const int rr = e % bc, c = e / bc;
+      const int src = ord[c];
+      const double sv_ = sig[src];
+      double v = 0.0;
+      if (rr < mu && sv_ > 0.0) v = Mm[rr + (int64_t)src * mu] / sv_;
+      Xo[rr + (int64_t)c * bc] = v;
+    }
+    __syncthreads();
+    // Vm_r (mv x r) = M0^T Um_r / sigma -> Yo (bk x r, rows >= mv zero)
+    for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+      const int rr = e % bk, c = e / bk;
+      double v = 0.0;
+      const double sv_ = sig[ord[c]];
+      if (rr < mv && sv_ > 0.0) {
+        for (int t = 0; t < mu; ++t) v += M0[t + (int64_t)rr * mu] * Xo[t + (int64_t)c * bc];
+        v /= sv_;
+      }
+      Yo[rr + (int64_t)c * bk] = v;
+    }
+    __syncthreads();
+    // U = Qu Xo ; Vt = Qv Yo
+    cta_apply_q(bc, mu, Ash, bc, tau_u, r, Xo, (int64_t)bc);
+    cta_apply_q(bk, mv, Bsh, bk, tau_v, r, Yo, (int64_t)bk);
+    for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+      const int rr = e % bc, c = e / bc;
+      Uc[rr + (int64_t)c * ld] = T(Xo[rr + (int64_t)c * bc]);
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+      const int rr = e % bk, c = e / bk;
+      Vc[rr + (int64_t)c * ld] = T(Yo[rr + (int64_t)c * bk]);
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
+      const int rr = e % r, c = e / r;
+      Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? sig[ord[c]] : 0.0);
+    }
+    if (threadIdx.x == 0) A.rank[blk] = r;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Solve kernels.  z is the n x nrhs right-hand side / solution (T, ld n).
+// Forward (trsm(L, b, Lower), trsm.cpp:163-174 for a block column B):
+//   y_i = Linv_i P_i z_i ; z_j -= L(j,i) y_i for j > i.
+// Backward (trsm(U, b, Upper), trsm.cpp:136-145):
+//   x_i = Uinv_i z_i ; z_j -= U(j,i) x_i for j < i.
+// ---------------------------------------------------------------------------
+constexpr int SOLVE_THREADS = 256;
+
+// y = M * P(z_i) (or M z_i), in place in z_i; M = Linv or Uinv; tmp (bmax x nrhs)
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, FactorWs<T> ws, int i, T* z, int64_t ldz,
+                                                              int nrhs, int which, T* tmp) {
+  // which: 0 forward (Linv, permute first), 1 backward (Uinv),
+  //        2 transpose-forward (Uinv^T), 3 transpose-backward (P^T Linv^T)
+  const int b = A.bs(i), ld = A.bmax;
+  const int64_t o = A.off[i];
+  const T* Mx = (which == 0 || which == 3) ? ws.Linv + (int64_t)i * ld * ld : ws.Uinv + (int64_t)i * ld * ld;
+  const int* perm = ws.perm + (int64_t)i * ld;
+  for (int e = threadIdx.x; e < b * nrhs; e += blockDim.x) {
+    const int r = e % b, c = e / b;
+    tmp[r + (int64_t)c * ld] = z[o + (which == 0 ? perm[r] : r) + (int64_t)c * ldz];
+  }
+  __syncthreads();
+  const bool tr = (which >= 2);
+  // row r of the result, per warp: lanes over the inner index
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int e = wid; e < b * nrhs; e += nw) {
+    const int r = e % b, c = e / b;
+    double s = 0.0;
+    for (int t = lane; t < b; t += 32) {
+      const double mv = tr ? double(Mx[t + (int64_t)r * ld]) : double(Mx[r + (int64_t)t * ld]);
+      s += mv * double(tmp[t + (int64_t)c * ld]);
+    }
+    s = warp_sum(s);
+    if (lane == 0) {
+      const int dst = (which == 3) ? perm[r] : r;
+      z[o + dst + (int64_t)c * ldz] = T(s);
+    }
+  }
+}
+
+// z_j -= Blk(j,i) * z_i for j in the target set (one CTA per target block j).
+// mode 0: targets j > i using blocks (j, i)        [forward, L]
+// mode 1: targets j < i using blocks (j, i)        [backward, U]
+// mode 2: targets j > i using blocks (i, j)^T      [transpose forward, U^T]
+// mode 3: targets j < i using blocks (i, j)^T      [transpose backward, L^T]
+template <typename T>
+__global__ void __launch_bounds__(SOLVE_THREADS) k_solve_scatter(BlrView<T> A, int i, T* z, int64_t ldz, int nrhs,
+                                                                 int mode, T* tmpbase) {
+  const int j = (mode == 0 || mode == 2) ? i + 1 + blockIdx.x : (int)blockIdx.x;
+  const int ld = A.bmax;
+  const int bj = A.bs(j), bi = A.bs(i);
+  const int64_t oj = A.off[j], oi = A.off[i];
+  const bool tr = (mode >= 2);
+  const int bi_ = tr ? i : j, bj_ = tr ? j : i;  // block (bi_, bj_)
+  T* tmp = tmpbase + (int64_t)blockIdx.x * ld * 8;  // kcap x nrhs (nrhs <= 8)
+  extern __shared__ double ssm[];  // kcap * nrhs doubles
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (A.is_lr(bi_, bj_)) {
+    const int r = A.rank[bi_ * A.nb + bj_];
+    const T* U = A.u(bi_, bj_);
+    const T* S = A.s(bi_, bj_);
+    const T* V = A.vt(bi_, bj_);
+    // non-transposed: z_j -= U S V^T z_i ; transposed: z_j -= V S^T U^T z_i
+    const T* inner = tr ? U : V;      // contracted with z_i (length bi)
+    const T* outer = tr ? V : U;      // expands to length bj
+    // t1 = inner^T z_i  (r x nrhs)
+    for (int e = wid; e < r * nrhs; e += nw) {
+      const int c = e % r, h = e / r;
+      double s = 0.0;
+      for (int t = lane; t < bi; t += 32) s += double(inner[t + (int64_t)c * ld]) * double(z[oi + t + (int64_t)h * ldz]);
+      s = warp_sum(s);
+      if (lane == 0) ssm[c + h * r] = s;
+    }
+    __syncthreads();
+    // t2 = S t1 (or S^T t1)
+    for (int e = threadIdx.x; e < r * nrhs; e += blockDim.x) {
+      const int c = e % r, h = e / r;
+      double s = 0.0;
+      for (int t = 0; t < r; ++t) {
+        const double sv = tr ? double(S[t + (int64_t)c * A.kcap]) : double(S[c + (int64_t)t * A.kcap]);
+        s += sv * ssm[t + h * r];
+      }
+      tmp[c + (int64_t)h * ld] = T(s);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < bj * nrhs; e += blockDim.x) {
+      const int rr = e % bj, h = e / bj;
+      double s = 0.0;
+      for (int t = 0; t < r; ++t) s += double(outer[rr + (int64_t)t * ld]) * double(tmp[t + (int64_t)h * ld]);
+      z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+    }
+  } else {
+    const T* Dm = A.dense(bi_, bj_);
+    for (int e = wid; e < bj * nrhs; e += nw) {
+      const int rr = e % bj, h = e / bj;
+      double s = 0.0;
+      for (int t = lane; t < bi; t += 32) {
+        const double dv = tr ? double(Dm[t + (int64_t)rr * ld]) : double(Dm[rr + (int64_t)t * ld]);
+        s += dv * double(z[oi + t + (int64_t)h * ldz]);
+      }
+      s = warp_sum(s);
+      if (lane == 0) z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K6: FP64 H-matvec partials: part[(i*nb + j)] = A(i,j) x_j  (bmax x nrhs each)
+// grid (nb, nb); then k_matvec_reduce sums over j in fixed order.
+// ---------------------------------------------------------------------------
+constexpr int MV_THREADS = 256;
+
+__global__ void __launch_bounds__(MV_THREADS) k_matvec_blocks(BlrView<double> H, const double* x, int64_t ldx,
+                                                              int nrhs, double* part) {
+  const int i = blockIdx.y, j = blockIdx.x;
+  const int nb = H.nb, ld = H.bmax;
+  const int bi = H.bs(i), bj = H.bs(j);
+  const int64_t oj = H.off[j];
+  double* out = part + (int64_t)(i * nb + j) * ld * nrhs;
+  extern __shared__ double t1[];   // 2 * kcap * nrhs doubles
+  double* t2 = t1 + (int64_t)H.kcap * nrhs;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (H.is_lr(i, j)) {
+    const int r = H.rank[i * nb + j];
+    const double* U = H.u(i, j);
+    const double* S = H.s(i, j);
+    const double* V = H.vt(i, j);
+    for (int e = wid; e < r * nrhs; e += nw) {
+      const int c = e % r, h = e / r;
+      double s = 0.0;
+      for (int t = lane; t < bj; t += 32) s += V[t + (int64_t)c * ld] * x[oj + t + (int64_t)h * ldx];
+      s = warp_sum(s);
+      if (lane == 0) t1[c + h * r] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < r * nrhs; e += blockDim.x) {
+      const int c = e % r, h = e / r;
+      double s = 0.0;
+      for (int t = 0; t < r; ++t) s += S[c + (int64_t)t * H.kcap] * t1[t + h * r];
+      t2[c + h * r] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+      const int rr = e % bi, h = e / bi;
+      double s = 0.0;
+      for (int t = 0; t < r; ++t) s += U[rr + (int64_t)t * ld] * t2[t + h * r];
+      out[rr + (int64_t)h * ld] = s;
+    }
+  } else {
+    const double* Dm = H.dense(i, j);
+    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+      const int rr = e % bi, h = e / bi;
+      double s = 0.0;
+      for (int t = 0; t < bj; ++t) s += Dm[rr + (int64_t)t * ld] * x[oj + t + (int64_t)h * ldx];
+      out[rr + (int64_t)h * ld] = s;
+    }
+  }
+}
+
+// y_i = sum_j part(i,j) (fixed order).  If b != null: y = b - A x (residual).
+__global__ void k_matvec_reduce(BlrView<double> H, const double* part, int nrhs, const double* bvec, int64_t ldb,
+                                double* y, int64_t ldy) {
+  const int i = blockIdx.x;
+  const int nb = H.nb, ld = H.bmax;
+  const int bi = H.bs(i);
+  const int64_t oi = H.off[i];
+  for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+    const int rr = e % bi, h = e / bi;
+    double s = 0.0;
+    for (int j = 0; j < nb; ++j) s += part[(int64_t)(i * nb + j) * ld * nrhs + rr + (int64_t)h * ld];
+    if (bvec) s = bvec[oi + rr + (int64_t)h * ldb] - s;
+    y[oi + rr + (int64_t)h * ldy] = s;
+  }
+}
+
+// column 2-norms squared of an n x nrhs matrix: per-CTA partials part[blk*nrhs + h]
+__global__ void k_colnorm2(const double* v, int64_t n, int64_t ldv, int nrhs, double* part) {
+  __shared__ double red[32];
+  for (int h = 0; h < nrhs; ++h) {
+    double s = 0.0;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+      const double a = v[r + h * ldv];
+      s += a * a;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) part[blockIdx.x * nrhs + h] = s;
+  }
+}
+
+template <typename TD, typename TS>
+__global__ void k_cast_copy(const TS* src, int64_t lds, TD* dst, int64_t ldd, int64_t n, int nrhs) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % n, h = e / n;
+    dst[r + h * ldd] = TD(src[r + h * lds]);
+  }
+}
+
+// x += T(d)
+template <typename TS>
+__global__ void k_axpy_cast(const TS* d, int64_t ldd, double* x, int64_t ldx, int64_t n, int nrhs) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % n, h = e / n;
+    x[r + h * ldx] += double(d[r + h * ldd]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Construction on the device (FP64): kernel evaluation and compression.
+// ---------------------------------------------------------------------------
+struct KernelDesc {
+  int kind;
+  int dim;
+  const double* x;   // dim x n, axis-major
+  int64_t n;
+  double p0, p1;
+};
+
+FRANK_D double kernel_eval(const KernelDesc& K, int64_t gi, int64_t gj) {
+  double r2 = 0.0;
+  for (int d = 0; d < K.dim; ++d) {
+    const double t = K.x[d * K.n + gi] - K.x[d * K.n + gj];
+    r2 += t * t;
+  }
+  const double r = sqrt(r2);
+  switch (K.kind) {
+    case 0: return 1.0 / (r + 1e-3);                                   // functions.cpp:92-109
+    case 1: return exp(-1.0 * r2) / (r + 1e-3);                        // functions.cpp:111-128
+    case 2: return -log(r + 1e-3) + (gi == gj ? K.p0 : 0.0);
+    default: return exp(-r / K.p0) + (gi == gj ? K.p1 : 0.0);
+  }
+}
+
+// Dense blocks of A_H: one CTA per dense block (listed in blocks[]).
+__global__ void k_build_dense(BlrView<double> H, KernelDesc K, const int* blocks, int nblocks) {
+  for (int t = blockIdx.x; t < nblocks; t += gridDim.x) {
+    const int blk = blocks[t];
+    const int i = blk / H.nb, j = blk % H.nb;
+    const int bi = H.bs(i), bj = H.bs(j);
+    double* Dm = H.dense(i, j);
+    for (int64_t e = threadIdx.x; e < (int64_t)bi * bj; e += blockDim.x) {
+      const int r = e % bi, c = e / bi;
+      Dm[r + (int64_t)c * H.bmax] = kernel_eval(K, H.off[i] + r, H.off[j] + c);
+    }
+  }
+}
+
+// Admissible blocks: evaluate, truncated column-pivoted QR to eps * ||A||_F
+// (operations/LAPACK/geqp3.cpp:71-192, LAWN 176 norm down-dating), Q by
+// applying the reflectors, R with columns permuted back, then RQ of R
+// (via QR of the column-reversed R^T) so S is upper triangular and V has
+// orthonormal rows (classes/low_rank.cpp:50-59).  One CTA per block, FP64
+// scratch per CTA slot: A (b x b), Q (b x b), X (b x b), norms, pivots.
+constexpr int BUILD_THREADS = 512;
+
+__global__ void __launch_bounds__(BUILD_THREADS) k_build_lowrank(BlrView<double> H, KernelDesc K, const int* blocks,
+                                                                 int nblocks, double eps, double* scratch,
+                                                                 int64_t stride, int* err) {
+  __shared__ double red[32];
+  __shared__ int redi[32];
+  const int ld = H.bmax;
+  double* base = scratch + (int64_t)blockIdx.x * stride;
+  double* Am = base;                               // b x b
+  double* Qm = Am + (int64_t)ld * ld;              // b x b
+  double* Xm = Qm + (int64_t)ld * ld;              // b x b
+  double* cnorm = Xm + (int64_t)ld * ld;           // b
+  double* partial = cnorm + ld;                    // b
+  double* tau = partial + ld;                      // b
+  double* tau2 = tau + ld;                         // b
+  int* jpvt = reinterpret_cast<int*>(tau2 + ld);   // b
+  int* jinv = jpvt + ld;                           // b
+  const double dlamch_e = 1.1102230246251565e-16;  // LAPACK dlamch('e') = eps/2 (rounding)
+  const double tol3z = sqrt(dlamch_e);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int t = blockIdx.x; t < nblocks; t += gridDim.x) {
+    const int blk = blocks[t];
+    const int i = blk / H.nb, j = blk % H.nb;
+    const int m = H.bs(i), n = H.bs(j);
+    const int mind = min(m, n);
+    for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+      const int r = e % m, c = e / m;
+      Am[r + (int64_t)c * m] = kernel_eval(K, H.off[i] + r, H.off[j] + c);
+    }
+    __syncthreads();
+    double fro = 0.0;
+    for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) fro += Am[e] * Am[e];
+    fro = block_sum(fro, red);
+    for (int c = wid; c < n; c += nw) {
+      double s = 0.0;
+      for (int r = lane; r < m; r += 32) s += Am[r + (int64_t)c * m] * Am[r + (int64_t)c * m];
+      s = warp_sum(s);
+      if (lane == 0) { cnorm[c] = sqrt(s); partial[c] = sqrt(s); jpvt[c] = c; }
+    }
+    __syncthreads();
+    const double threshold = eps * sqrt(fro);
+    double maxc;
+    {
+      double best = -1.0; int bi = -1;
+      for (int c = threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+      block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+    }
+    int r = 0;
+    if (maxc <= dlamch_e) {
+      // zero block: Q = e_0, R = 0 (geqp3.cpp:97-102)
+      for (int e = threadIdx.x; e < m; e += blockDim.x) H.u(i, j)[e] = (e == 0) ? 1.0 : 0.0;
+      for (int e = threadIdx.x; e < n; e += blockDim.x) H.vt(i, j)[e] = (e == 0) ? 1.0 : 0.0;
+      if (threadIdx.x == 0) { H.s(i, j)[0] = 0.0; H.rank[blk] = 1; }
+      __syncthreads();
+      continue;
+    }
+    while (r < mind && maxc > threshold) {
+      // pivot: first max over cnorm[r..n)
+      double best = -1.0; int bi = -1;
+      for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+      double dummy;
+      const int kp = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &dummy);
+      if (kp != r) {
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {
+          const double a = Am[e + (int64_t)r * m];
+          Am[e + (int64_t)r * m] = Am[e + (int64_t)kp * m];
+          Am[e + (int64_t)kp * m] = a;
+        }
+        if (threadIdx.x == 0) {
+          double a = cnorm[r]; cnorm[r] = cnorm[kp]; cnorm[kp] = a;
+          a = partial[r]; partial[r] = partial[kp]; partial[kp] = a;
+          int q = jpvt[r]; jpvt[r] = jpvt[kp]; jpvt[kp] = q;
+        }
+      }
+      __syncthreads();
+      // reflector on column r, rows r..m-1 (dlarfg)
+      double* col = Am + (int64_t)r * m;
+      double s = 0.0;
+      for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) s += col[e] * col[e];
+      const double xn2 = block_sum(s, red);
+      const double alpha = col[r];
+      double tt = 0.0, beta = alpha, scal = 0.0;
+      if (xn2 > 0.0) {
+        const double nrm = sqrt(alpha * alpha + xn2);
+        beta = alpha >= 0.0 ? -nrm : nrm;
+        tt = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+        for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) col[e] *= scal;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) { col[r] = beta; tau[r] = tt; }
+      __syncthreads();
+      if (r < mind - 1 && tt != 0.0) {
+        for (int c = r + 1 + wid; c < n; c += nw) {
+          double* cc = Am + (int64_t)c * m;
+          double w = (lane == 0) ? cc[r] : 0.0;
+          for (int e = r + 1 + lane; e < m; e += 32) w += col[e] * cc[e];
+          w = warp_sum(w) * tt;
+          if (lane == 0) cc[r] -= w;
+          for (int e = r + 1 + lane; e < m; e += 32) cc[e] -= w * col[e];
+        }
+      }
+      __syncthreads();
+      // norm down-date (geqp3.cpp:137-159)
+      for (int c = r + 1 + wid; c < n; c += nw) {
+        if (cnorm[c] != 0.0) {
+          double temp = fabs(Am[r + (int64_t)c * m] / cnorm[c]);
+          temp = fmax(0.0, (1.0 - temp) * (1.0 + temp));
+          const double ratio = cnorm[c] / partial[c];
+          const double temp2 = temp * ratio * ratio;
+          if (temp2 > tol3z) {
+            if (lane == 0) cnorm[c] = cnorm[c] * sqrt(temp);
+          } else {
+            double s2 = 0.0;
+            if (r < m - 1)
+              for (int e = r + 1 + lane; e < m; e += 32) s2 += Am[e + (int64_t)c * m] * Am[e + (int64_t)c * m];
+            s2 = warp_sum(s2);
+            if (lane == 0) { cnorm[c] = (r < m - 1) ? sqrt(s2) : 0.0; partial[c] = cnorm[c]; }
+          }
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      ++r;
+      best = -1.0; bi = -1;
+      for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+      block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+      if (r >= n) maxc = 0.0;
+    }
+    if (r > H.kcap) { if (threadIdx.x == 0) atomicAdd(err + ERR_RANK_OVERFLOW, 1); }
+    // Q (m x r) = H_0..H_{r-1} [I_r; 0]
+    for (int64_t e = threadIdx.x; e < (int64_t)m * r; e += blockDim.x) {
+      const int rr = e % m, c = e / m;
+      Qm[rr + (int64_t)c * m] = (rr == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    cta_apply_q(m, r, Am, m, tau, r, Qm, (int64_t)m);
+    // inverse pivot: R_perm[:, jpvt[c]] = R[:, c]; build X = (R_perm)^T reversed columns:
+    // X (n x r): X[c, a] = R_perm[r-1-a, c]
+    for (int c = threadIdx.x; c < n; c += blockDim.x) jinv[jpvt[c]] = c;
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (int64_t)n * r; e += blockDim.x) {
+      const int c = e % n, a = e / n;
+      const int row = r - 1 - a;
+      const int src = jinv[c];
+      Xm[c + (int64_t)a * n] = (row <= src) ? Am[row + (int64_t)src * m] : 0.0;
+    }
+    __syncthreads();
+    // QR of X (n x r): X = Qt Rt; S = J Rt^T J, Vt[:, a] = Qt[:, r-1-a]
+    cta_householder_qr(n, r, Xm, n, tau2, red);
+    const int rs = min(r, H.kcap);
+    double* Sd = H.s(i, j);
+    for (int64_t e = threadIdx.x; e < (int64_t)rs * rs; e += blockDim.x) {
+      const int a = e % rs, c = e / rs;
+      // S[a][c] = Rt[r-1-c][r-1-a] (upper triangular in (a, c))
+      const int ra = r - 1 - c, ca = r - 1 - a;
+      Sd[a + (int64_t)c * H.kcap] = (ra <= ca) ? Xm[ra + (int64_t)ca * n] : 0.0;
+    }
+    // explicit Qt (n x r) into Qm's second half? reuse Am (no longer needed)
+    double* Qt = Am;
+    for (int64_t e = threadIdx.x; e < (int64_t)n * r; e += blockDim.x) {
+      const int rr = e % n, c = e / n;
+      Qt[rr + (int64_t)c * n] = (rr == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    cta_apply_q(n, r, Xm, n, tau2, r, Qt, (int64_t)n);
+    double* Ud = H.u(i, j);
+    double* Vd = H.vt(i, j);
+    for (int64_t e = threadIdx.x; e < (int64_t)m * rs; e += blockDim.x) {
+      const int rr = e % m, c = e / m;
+      Ud[rr + (int64_t)c * ld] = Qm[rr + (int64_t)c * m];
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)n * rs; e += blockDim.x) {
+      const int rr = e % n, a = e / n;
+      Vd[rr + (int64_t)a * ld] = Qt[rr + (int64_t)(r - 1 - a) * n];
+    }
+    if (threadIdx.x == 0) H.rank[blk] = rs;
+    __syncthreads();
+  }
+}
+
+}  // namespace frank

@@ -1,0 +1,293 @@
+// Device helpers shared by the BLR-LU kernels: reductions, a CTA-wide tiled
+// GEMM on column-major operands, Householder QR / Q application, and a
+// one-sided Jacobi SVD.  Every routine here is executed cooperatively by all
+// threads of one thread block (CTA) and ends with a __syncthreads().
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#define FRANK_HD __host__ __device__ __forceinline__
+#define FRANK_D __device__ __forceinline__
+
+namespace frank {
+
+// Error word layout (device int array of the plan).
+enum ErrSlot {
+  ERR_SINGULAR_STEP = 0,   // 1 + first block step whose getrf met a zero pivot
+  ERR_RANK_OVERFLOW = 1,   // count of recompressions clamped at the capacity
+  ERR_JACOBI = 2,          // count of core SVDs that hit the sweep limit
+  ERR_BOUNDS = 3,          // count of index checks that failed (skipped access)
+  ERR_MAX_RANK = 4,        // largest rank produced by a recompression
+  ERR_RECOMP = 5,          // recompressions performed (low 31 bits)
+  ERR_SLOTS = 8
+};
+
+FRANK_D double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+FRANK_D float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the CTA; `red` is shared scratch of >= 32 doubles.  All threads
+// receive the result.
+FRANK_D double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = (threadIdx.x < (unsigned)nw) ? red[threadIdx.x] : 0.0;
+  if (wid == 0) t = warp_sum(t);
+  if (threadIdx.x == 0) red[0] = t;
+  __syncthreads();
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// Arg-max of |v| over the CTA with ties broken toward the smallest index
+// (LAPACK idamax semantics).  Returns the index; *absval gets the value.
+FRANK_D int block_argmax_abs(double v, int idx, double* redv, int* redi, double* absval) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  double a = fabs(v);
+  if (idx < 0) a = -1.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double oa = __shfl_xor_sync(0xffffffffu, a, o);
+    int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (oa > a || (oa == a && oi >= 0 && (idx < 0 || oi < idx))) { a = oa; idx = oi; }
+  }
+  __syncthreads();
+  if (lane == 0) { redv[wid] = a; redi[wid] = idx; }
+  __syncthreads();
+  if (wid == 0) {
+    a = (lane < nw) ? redv[lane] : -1.0;
+    idx = (lane < nw) ? redi[lane] : -1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double oa = __shfl_xor_sync(0xffffffffu, a, o);
+      int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+      if (oa > a || (oa == a && oi >= 0 && (idx < 0 || oi < idx))) { a = oa; idx = oi; }
+    }
+    if (lane == 0) { redv[0] = a; redi[0] = idx; }
+  }
+  __syncthreads();
+  int r = redi[0];
+  *absval = redv[0];
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// CTA-wide GEMM: C(m x n) = alpha * op(A) * op(B) + beta * C, column-major.
+// op(A) is m x k: A is (m x k, lda) when !ta, (k x m, lda) when ta.
+// op(B) is k x n: B is (k x n, ldb) when !tb, (n x k, ldb) when tb.
+// beta == 0 never reads C.  64x64 output tiles, k in steps of 16, operands
+// staged through shared memory in the accumulate type.  `smem` must hold
+// 2 * 16 * 64 TACC values.  Requires blockDim.x == NT (256 or 512).
+// ---------------------------------------------------------------------------
+template <typename TACC, int NT, typename TA, typename TB, typename TC>
+FRANK_D void cta_gemm(int m, int n, int k, TACC alpha, const TA* __restrict__ A, int64_t lda, bool ta,
+                      const TB* __restrict__ B, int64_t ldb, bool tb, TACC beta, TC* C, int64_t ldc,
+                      TACC* smem) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+  constexpr int TM = 4, TN = (NT == 256) ? 4 : 2;
+  static_assert((BM / TM) * (BN / TN) == NT, "tile/threads mismatch");
+  TACC* As = smem;            // [BK][BM]
+  TACC* Bs = smem + BK * BM;  // [BK][BN]
+  const int tid = threadIdx.x;
+  const int tr = tid % (BM / TM);   // row group
+  const int tc = tid / (BM / TM);   // col group
+  if (m <= 0 || n <= 0) { __syncthreads(); return; }
+  for (int r0 = 0; r0 < m; r0 += BM) {
+    for (int c0 = 0; c0 < n; c0 += BN) {
+      TACC acc[TM][TN];
+#pragma unroll
+      for (int a = 0; a < TM; ++a)
+#pragma unroll
+        for (int b = 0; b < TN; ++b) acc[a][b] = TACC(0);
+      for (int k0 = 0; k0 < k; k0 += BK) {
+        for (int idx = tid; idx < BM * BK; idx += NT) {
+          int rr, kk;
+          if (!ta) { rr = idx % BM; kk = idx / BM; } else { kk = idx % BK; rr = idx / BK; }
+          const int gr = r0 + rr, gk = k0 + kk;
+          TACC v = TACC(0);
+          if (gr < m && gk < k) v = ta ? TACC(A[gk + (int64_t)gr * lda]) : TACC(A[gr + (int64_t)gk * lda]);
+          As[kk * BM + rr] = v;
+        }
+        for (int idx = tid; idx < BN * BK; idx += NT) {
+          int cc, kk;
+          if (!tb) { kk = idx % BK; cc = idx / BK; } else { cc = idx % BN; kk = idx / BN; }
+          const int gc = c0 + cc, gk = k0 + kk;
+          TACC v = TACC(0);
+          if (gc < n && gk < k) v = tb ? TACC(B[gc + (int64_t)gk * ldb]) : TACC(B[gk + (int64_t)gc * ldb]);
+          Bs[kk * BN + cc] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+          TACC av[TM], bv[TN];
+#pragma unroll
+          for (int a = 0; a < TM; ++a) av[a] = As[kk * BM + tr + a * (BM / TM)];
+#pragma unroll
+          for (int b = 0; b < TN; ++b) bv[b] = Bs[kk * BN + tc + b * (BN / TN)];
+#pragma unroll
+          for (int a = 0; a < TM; ++a)
+#pragma unroll
+            for (int b = 0; b < TN; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int a = 0; a < TM; ++a) {
+        const int gr = r0 + tr + a * (BM / TM);
+        if (gr >= m) continue;
+#pragma unroll
+        for (int b = 0; b < TN; ++b) {
+          const int gc = c0 + tc + b * (BN / TN);
+          if (gc >= n) continue;
+          TC* p = C + gr + (int64_t)gc * ldc;
+          TACC v = alpha * acc[a][b];
+          if (beta != TACC(0)) v += beta * TACC(*p);
+          *p = TC(v);
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Householder QR (LAPACK dgeqr2 / dlarfg conventions) of the column-major
+// m x n matrix A (lda) in FP64, in place: R on and above the diagonal, the
+// reflector vectors v (v_0 = 1 implicit) below, tau[min(m,n)].
+// Warps take columns, lanes take rows.
+// ---------------------------------------------------------------------------
+FRANK_D void cta_householder_qr(int m, int n, double* A, int64_t lda, double* tau, double* red) {
+  const int kmin = m < n ? m : n;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = 0; j < kmin; ++j) {
+    double* col = A + (int64_t)j * lda;
+    double s = 0.0;
+    for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) s += col[r] * col[r];
+    const double xnorm2 = block_sum(s, red);
+    const double alpha = col[j];
+    double t = 0.0, beta = alpha, scal = 0.0;
+    if (xnorm2 > 0.0) {
+      const double nrm = sqrt(alpha * alpha + xnorm2);
+      beta = alpha >= 0.0 ? -nrm : nrm;
+      t = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    // scale v and set the diagonal
+    if (xnorm2 > 0.0)
+      for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) col[r] *= scal;
+    __syncthreads();
+    if (threadIdx.x == 0) { col[j] = beta; tau[j] = t; }
+    __syncthreads();
+    if (t != 0.0) {
+      // apply H = I - t v v^T to columns j+1..n-1
+      for (int c = j + 1 + wid; c < n; c += nw) {
+        double* cc = A + (int64_t)c * lda;
+        double w = 0.0;
+        if (lane == 0) w = cc[j];
+        for (int r = j + 1 + lane; r < m; r += 32) w += col[r] * cc[r];
+        w = warp_sum(w) * t;
+        if (lane == 0) cc[j] -= w;
+        for (int r = j + 1 + lane; r < m; r += 32) cc[r] -= w * col[r];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// X (m x r, ldx) := Q X where Q = H_0 H_1 ... H_{k-1} from cta_householder_qr
+// (reflectors in V, m x k, ldv).  LAPACK dorm2r, left, no transpose.
+template <typename TX>
+FRANK_D void cta_apply_q(int m, int k, const double* V, int64_t ldv, const double* tau,
+                         int r, TX* X, int64_t ldx) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = k - 1; j >= 0; --j) {
+    const double t = tau[j];
+    if (t != 0.0) {
+      const double* v = V + (int64_t)j * ldv;
+      for (int c = wid; c < r; c += nw) {
+        TX* xc = X + (int64_t)c * ldx;
+        double w = 0.0;
+        if (lane == 0) w = double(xc[j]);
+        for (int i = j + 1 + lane; i < m; i += 32) w += v[i] * double(xc[i]);
+        w = warp_sum(w) * t;
+        if (lane == 0) xc[j] = TX(double(xc[j]) - w);
+        for (int i = j + 1 + lane; i < m; i += 32) xc[i] = TX(double(xc[i]) - w * v[i]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One-sided (Hestenes) Jacobi on the columns of G (m x n, ldg), FP64, in
+// place: on return the columns are mutually orthogonal, G = U * Sigma
+// (unsorted).  Pairs are scheduled by the round-robin (circle) method so a
+// round's pairs are disjoint; each warp rotates one pair at a time.
+// Rotation: zeta = (beta - alpha) / (2 gamma), t = sign(zeta) /
+// (|zeta| + sqrt(1 + zeta^2)), c = 1/sqrt(1+t^2), s = c t (Demmel & Veselic,
+// "Jacobi's method is more accurate than QR", 1992).  Returns the number of
+// sweeps, or -1 if max_sweeps was reached without convergence.
+// ---------------------------------------------------------------------------
+FRANK_D int cta_jacobi_columns(int m, int n, double* G, int64_t ldg, int max_sweeps, int* flag) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int N2 = n + (n & 1);
+  const double tol = (double)(m > 1 ? m : 1) * 2.220446049250313e-16;
+  if (n < 2) { __syncthreads(); return 0; }
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    if (threadIdx.x == 0) *flag = 0;
+    __syncthreads();
+    for (int round = 0; round < N2 - 1; ++round) {
+      for (int pr = wid; pr < N2 / 2; pr += nw) {
+        int p, q;
+        if (pr == 0) { p = N2 - 1; q = round; }
+        else { p = (round + pr) % (N2 - 1); q = (round - pr + N2 - 1) % (N2 - 1); }
+        if (p >= n || q >= n) continue;
+        if (p > q) { int t = p; p = q; q = t; }
+        double* gp = G + (int64_t)p * ldg;
+        double* gq = G + (int64_t)q * ldg;
+        double a = 0.0, b = 0.0, g = 0.0;
+        for (int i = lane; i < m; i += 32) {
+          const double x = gp[i], y = gq[i];
+          a = fma(x, x, a); b = fma(y, y, b); g = fma(x, y, g);
+        }
+        a = warp_sum(a); b = warp_sum(b); g = warp_sum(g);
+        if (a == 0.0 || b == 0.0) continue;
+        if (fabs(g) <= tol * sqrt(a) * sqrt(b)) continue;
+        const double zeta = (b - a) / (2.0 * g);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t);
+        const double s = c * t;
+        for (int i = lane; i < m; i += 32) {
+          const double x = gp[i], y = gq[i];
+          gp[i] = c * x - s * y;
+          gq[i] = s * x + c * y;
+        }
+        if (lane == 0) *flag = 1;
+      }
+      __syncthreads();
+    }
+    const int rotated = *flag;
+    __syncthreads();
+    if (!rotated) return sweep + 1;
+  }
+  return -1;
+}
+
+}  // namespace frank

@@ -1,0 +1,175 @@
+/*
+ * frank_b200.h -- C ABI of the B200 engine for FRANK's BLR-LU
+ * factor-and-solve path.
+ *
+ * Plain pointers and sizes only; no torch or CUDA types cross this boundary
+ * (streams are passed as `void*` holding a cudaStream_t, NULL = default).
+ * Host buffers are ordinary host memory (pinned or not); `_device` variants
+ * take device pointers.
+ *
+ * Each entry point names the FRANK interface it replaces (paths within the
+ * FRANK project).  A plan ("frank_blr") is one block-low-rank matrix resident
+ * on one GPU: the FP64 compressed matrix A_H (kept for the residual of
+ * iterative refinement) plus a working copy in the factorization precision
+ * that getrf overwrites with its L and U factors.
+ *
+ * Thread safety: a plan is not thread-safe; distinct plans may be used from
+ * distinct host threads.  The library keeps no other mutable global state
+ * apart from the per-thread error string.
+ */
+#ifndef FRANK_B200_H
+#define FRANK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes returned by every entry point. */
+enum {
+  FRANK_OK = 0,
+  FRANK_ERR_INVALID = 1,        /* bad argument (see frank_last_error) */
+  FRANK_ERR_SINGULAR = 2,       /* a leaf getrf met an exactly zero pivot */
+  FRANK_ERR_UNSUPPORTED = 3,    /* block-type combination not supported */
+  FRANK_ERR_NOT_CONVERGED = 4,  /* refinement did not reach the tolerance */
+  FRANK_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
+  FRANK_ERR_CUDA = 6,           /* a CUDA runtime call failed */
+  FRANK_ERR_RANK_OVERFLOW = 7,  /* a recompressed rank exceeded the capacity */
+  FRANK_ERR_STATE = 8           /* call out of order (e.g. solve before getrf) */
+};
+
+/* Arithmetic of the factorization (the refinement residual is always FP64). */
+enum {
+  FRANK_PREC_FP64 = 0,   /* plain FP64 factor */
+  FRANK_PREC_MIXED = 1   /* FP32 bulk factor, FP64 leaf getrf / core SVD */
+};
+
+/* Block types (classes/dense.h, classes/low_rank.h). */
+enum { FRANK_BLOCK_DENSE = 0, FRANK_BLOCK_LOWRANK = 1 };
+
+/* Kernel functions for on-device construction (functions.cpp:92-128 and the
+ * two kernels of the batched / adjoint workloads). */
+enum {
+  FRANK_KERNEL_LAPLACE = 0,     /* 1/(r+1e-3)                  functions.cpp:92-109 */
+  FRANK_KERNEL_HELMHOLTZ = 1,   /* exp(-r^2)/(r+1e-3)          functions.cpp:111-128 */
+  FRANK_KERNEL_NEGLOG = 2,      /* -log(r+1e-3) + p0*delta_ij  */
+  FRANK_KERNEL_EXP = 3          /* exp(-r/p0) + p1*delta_ij    */
+};
+
+typedef struct frank_blr frank_blr;
+
+typedef struct frank_blr_desc {
+  int64_t n;          /* matrix order */
+  int32_t nb;         /* blocks per side; block sizes follow IndexRange::split
+                         (index_range.cpp:15-24): ceil(n/nb), last takes the rest */
+  int32_t max_rank;   /* rank capacity of every low-rank block (0 = block size) */
+  int32_t precision;  /* FRANK_PREC_* */
+  int32_t fixed_rank; /* >0: recompress to this rank (LowRank fixed-rank mode);
+                         0: truncate by eps (find_svd_truncation_rank, misc.cpp:133-146) */
+  double eps;         /* truncation tolerance of the factorization */
+  double admis;       /* position-based admissibility: block (i,j) is low rank
+                         iff |i - j| > admis (matrix_initializer.cpp:51-58);
+                         diagonal blocks are always dense */
+} frank_blr_desc;
+
+/* Text of the last error on the calling thread ("" if none). */
+const char* frank_last_error(void);
+
+/* Library / device information: compiled arch, device name, SM count. */
+int frank_device_info(char* name, int name_len, int* sm_count, int* cc_major, int* cc_minor);
+
+/* Create a plan on the current CUDA device.  Replaces the allocation side of
+ * Hierarchical(n_row_blocks, n_col_blocks) (classes/hierarchical.cpp:46-47). */
+int frank_blr_create(const frank_blr_desc* desc, frank_blr** out);
+
+/* Free all device memory of the plan. */
+int frank_blr_destroy(frank_blr* plan);
+
+/* Block geometry: offsets[nb+1] of the block rows/columns. */
+int frank_blr_offsets(const frank_blr* plan, int64_t* offsets);
+
+/* Set block (i, j) of A_H to a dense matrix (host, FP64).  `rowmajor` selects
+ * the layout of `a` with leading dimension `ld`.  Replaces
+ * MatrixInitializer::get_dense_representation (matrix_initializer.cpp:28-34). */
+int frank_blr_set_dense(frank_blr* plan, int i, int j, const double* a, int64_t ld, int rowmajor);
+
+/* Set block (i, j) of A_H to U (m x k) S (k x k) V (k x n), host FP64.
+ * Replaces LowRank(U, S, V) (classes/low_rank.cpp:61-69). */
+int frank_blr_set_lowrank(frank_blr* plan, int i, int j, int rank,
+                          const double* U, int64_t ldu, const double* S, int64_t lds,
+                          const double* V, int64_t ldv, int rowmajor);
+
+/* Build A_H on the device from points (dim x n, axis-major like the
+ * reference's params[d][i], functions.h:34-38): diagonal and inadmissible
+ * blocks dense, admissible blocks compressed by truncated column-pivoted QR
+ * + RQ (LowRank(Dense, eps), low_rank.cpp:50-59 with geqp3.cpp:71-192) when
+ * eps > 0.  Which blocks are low rank follows the plan's admissibility.
+ * kparams: kernel parameters (see FRANK_KERNEL_*), may be NULL.  Replaces
+ * Hierarchical(kernel, params, n, n, nleaf, eps, admis, nb, nb)
+ * (classes/hierarchical.cpp:89-109) for one level. */
+int frank_blr_build_kernel(frank_blr* plan, int kernel, const double* points, int dim,
+                           const double* kparams, double eps, void* stream);
+
+/* Block type and rank of block (i, j); which = 0: A_H, 1: working/factor. */
+int frank_blr_block_info(const frank_blr* plan, int which, int i, int j, int* type, int* rank);
+
+/* Copy block (i, j) of A_H (which=0) or of the factor (which=1) to host FP64.
+ * Dense: a (rows x cols, ld).  Low rank: U (m x rank), S (rank x rank),
+ * V (rank x n).  For which=1 after getrf: diagonal blocks hold the packed
+ * pivoted LU (unit L below, U on and above the diagonal) with pivots from
+ * frank_blr_get_pivots; blocks below the diagonal hold L, above hold U. */
+int frank_blr_get_dense(const frank_blr* plan, int which, int i, int j, double* a, int64_t ld, int rowmajor);
+int frank_blr_get_lowrank(const frank_blr* plan, int which, int i, int j,
+                          double* U, int64_t ldu, double* S, int64_t lds,
+                          double* V, int64_t ldv, int rowmajor);
+
+/* LAPACK-style 1-based pivot rows of the diagonal block i (after getrf). */
+int frank_blr_get_pivots(const frank_blr* plan, int i, int* ipiv);
+
+/* Right-looking block LU in place.  Replaces getrf(Hierarchical&)
+ * (operations/LAPACK/getrf.cpp:40-65) with its leaf getrf (getrf.cpp:67-84,
+ * here with partial pivoting applied), trsm (operations/BLAS/trsm.cpp:92-115),
+ * gemm (operations/BLAS/gemm.cpp:180-272) and rounded LowRank addition
+ * (operations/arithmetic/addition.cpp:93-127).  Resets the working copy from
+ * A_H first, so it may be called repeatedly. */
+int frank_blr_getrf(frank_blr* plan, void* stream);
+
+/* x = U^{-1} L^{-1} P b for nrhs right-hand sides (column-major n x nrhs,
+ * leading dimension ldb), in place.  Replaces trsm(L, b, Lower) followed by
+ * trsm(U, b, Upper) (trsm.cpp:117-125, 40-90; examples/h_lu.cpp:45-48). */
+int frank_blr_solve(frank_blr* plan, double* b, int64_t ldb, int nrhs, void* stream);
+int frank_blr_solve_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
+
+/* y = A_H x in FP64 (column-major, nrhs columns).  Replaces
+ * gemm(Hierarchical, Dense, Dense, 1, 0) (gemm.cpp:581-615). */
+int frank_blr_matvec(frank_blr* plan, const double* x, int64_t ldx, double* y, int64_t ldy,
+                     int nrhs, void* stream);
+int frank_blr_matvec_device(frank_blr* plan, const double* d_x, int64_t ldx, double* d_y,
+                            int64_t ldy, int nrhs, void* stream);
+
+/* Solve A_H x = b to a relative residual max_j ||b_j - A_H x_j|| / ||b_j|| <= tol
+ * by iterative refinement preconditioned with the factor (getrf must have run):
+ * x0 = (LU)^{-1} b, x += (LU)^{-1}(b - A_H x) with the residual in FP64.
+ * Reports iterations and the final relative residual.  Returns
+ * FRANK_ERR_NOT_CONVERGED if maxit is reached first. */
+int frank_blr_refine(frank_blr* plan, const double* b, int64_t ldb, double* x, int64_t ldx,
+                     int nrhs, double tol, int maxit, int* iters, double* resid, void* stream);
+int frank_blr_refine_device(frank_blr* plan, const double* d_b, int64_t ldb, double* d_x,
+                            int64_t ldx, int nrhs, double tol, int maxit, int* iters,
+                            double* resid, void* stream);
+
+/* Transposed solve x = (P^T L U)^{-T} b = A^{-T} b with the same factors, for
+ * the adjoint of solve(A, b) (no reference counterpart; python/FRANK adjoint). */
+int frank_blr_solve_transpose_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
+
+/* Counters of the last getrf: kernel launches issued, and the sum over all
+ * recompressions of (rank before, rank after) for reporting. */
+int frank_blr_stats(const frank_blr* plan, int64_t* launches, int64_t* recompressions,
+                    int64_t* max_rank_seen, int64_t* rank_overflows);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FRANK_B200_H */

@@ -343,9 +343,8 @@ def truncated_geqp3(A0: np.ndarray, eps: float):
             A[r + 1:, r] = x
             tau[r] = t
         else:
-            beta, x, t = lapack.dlarfg(1, A[r, r], np.zeros(0))
-            A[r, r] = beta
-            tau[r] = t
+            # dlarfg with n = 1 is the identity reflector: tau = 0, beta = alpha
+            tau[r] = 0.0
         if r < min_dim - 1:
             arr = A[r, r]
             A[r, r] = 1.0

@@ -1,0 +1,138 @@
+"""GPU parity of the BLR-LU path through the C ABI against the oracle, on the
+reference's own test grids (blr_fixed_acc_test, blr_fixed_rank_test) and a
+fixed-rank case of the N=2048 Laplace-1D workload.  Tolerances: the
+reference's own criteria (solve error <= eps), plus factorization error and
+solve error within a factor 10 of the oracle's at the same tolerance/rank."""
+import numpy as np
+import pytest
+
+import oracle.frank_oracle as fo
+
+pytestmark = pytest.mark.gpu
+FACTOR = 10.0
+
+
+def _upload(H, n, nb, **kw):
+    from frank_b200 import upload_hierarchical
+    return upload_hierarchical([[H[i, j] for j in range(nb)] for i in range(nb)], n, nb, **kw)
+
+
+def _factor_error(A_dense, M):
+    """||A - Lhat U||_F / ||A||_F from the downloaded factor blocks (pivots applied)."""
+    nb, off = M.nb, M.offsets
+    n = A_dense.shape[0]
+    L = np.zeros((n, n)); U = np.zeros((n, n))
+    for i in range(nb):
+        for j in range(nb):
+            r0, r1, c0, c1 = off[i], off[i + 1], off[j], off[j + 1]
+            blk = M.block_dense(i, j, which=1)
+            if i == j:
+                Li = np.tril(blk, -1) + np.eye(r1 - r0)
+                piv = M.pivots(i) - 1
+                perm = np.arange(r1 - r0)
+                for k, p in enumerate(piv):
+                    perm[[k, p]] = perm[[p, k]]
+                P = np.eye(r1 - r0)[perm]          # P A = L U  ->  A = P^T L U
+                L[r0:r1, c0:c1] = P.T @ Li
+                U[r0:r1, c0:c1] = np.triu(blk)
+            elif i > j:
+                L[r0:r1, c0:c1] = blk
+            else:
+                U[r0:r1, c0:c1] = blk
+    return np.linalg.norm(A_dense - L @ U) / np.linalg.norm(A_dense)
+
+
+GRID = [(n, eps, admis) for n in (128, 256) for eps in (1e-6, 1e-8, 1e-10) for admis in (0.0, 1.0, 4.0)]
+
+
+@pytest.mark.parametrize("n,eps,admis", GRID)
+def test_blr_fixed_accuracy_lu_matches_oracle(gpu_lib, n, eps, admis):
+    nb = n // 32
+    x = np.array([fo.get_sorted_random_vector(n)])
+    A = fo.build_hierarchical(fo.laplacend, x, n, 32, nb, eps=eps, admis=admis)
+    A_dense = fo.to_dense(A)
+    xv = fo.random_uniform(n, 1)
+    b = fo.matvec(A, xv)
+    M = _upload(A, n, nb, eps=eps, admis=admis)
+    # H-matvec parity (FP64)
+    np.testing.assert_allclose(M.matvec(xv), b, rtol=0, atol=1e-13 * np.abs(b).max())
+    L, U = fo.getrf(fo.deep_copy(A))
+    ref_solve = fo.l2_error(xv, fo.solve(L, U, b))
+    ref_ferr = np.linalg.norm(A_dense - fo.to_dense(L) @ fo.to_dense(U)) / np.linalg.norm(A_dense)
+    M.getrf()
+    gpu_solve = fo.l2_error(xv, M.solve(b))
+    gpu_ferr = _factor_error(A_dense, M)
+    assert gpu_solve <= eps                                   # blr_fixed_acc_test.cpp:82
+    assert gpu_solve <= FACTOR * ref_solve + 1e-14
+    assert gpu_ferr <= FACTOR * ref_ferr + 1e-14
+    # step-0 leaf factor is bitwise-close to the oracle's (same input)
+    np.testing.assert_allclose(np.triu(M.block(0, 0, which=1)), U[0, 0], rtol=0,
+                               atol=1e-12 * np.abs(U[0, 0]).max())
+
+
+def test_fixed_rank_laplace1d_2048(gpu_lib):
+    """N=2048 sorted points, 8x8 blocks of 256, rank 16 (rsvd construction,
+    fixed-rank rounded addition), FP64 factor + solve vs the oracle and the
+    dense LAPACK solve."""
+    n, nb, rank = 2048, 8, 16
+    x = np.array([fo.get_sorted_random_vector(n)])
+    A = fo.build_hierarchical(fo.laplacend, x, n, 256, nb, rank=rank)
+    A_dense = fo.to_dense(A)
+    rng = np.random.default_rng(1)
+    bv = rng.standard_normal((n, 1))
+    L, U = fo.getrf(fo.deep_copy(A))
+    xo = fo.solve(L, U, bv)
+    xd = np.linalg.solve(A_dense, bv)
+    M = _upload(A, n, nb, fixed_rank=rank)
+    M.getrf()
+    xg = M.solve(bv)
+    ref_err = np.linalg.norm(xo - xd) / np.linalg.norm(xd)
+    gpu_err = np.linalg.norm(xg - xd) / np.linalg.norm(xd)
+    assert gpu_err <= FACTOR * ref_err + 1e-13
+    for i in range(nb):
+        for j in range(nb):
+            if i != j:
+                assert M.rank(i, j, which=1) == rank
+
+
+@pytest.mark.parametrize("n,eps", [(256, 1e-8), (512, 1e-6)])
+def test_device_construction_matches_oracle(gpu_lib, n, eps):
+    """frank_blr_build_kernel vs LowRank(Dense, eps) of the oracle:
+    compression error <= eps (blr_fixed_acc_test.cpp:46-54) and ranks within 2."""
+    from frank_b200 import BLRMatrix
+    nb = n // 32
+    x = np.array([fo.get_sorted_random_vector(n)])
+    A = fo.build_hierarchical(fo.laplacend, x, n, 32, nb, eps=eps)
+    D = fo.laplacend(x, 0, n, 0, n)
+    M = BLRMatrix(n, nb, eps=eps)
+    M.build_kernel("laplace", x, eps)
+    G = M.to_dense()
+    assert fo.l2_error(D, G) <= eps
+    for i in range(nb):
+        for j in range(nb):
+            if i != j:
+                assert abs(M.rank(i, j) - A[i, j].rank) <= 2
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_mixed_precision_refinement_reaches_1e10(gpu_lib, dim):
+    """FP32 factor at a looser tolerance + FP64 refinement against the FP64
+    compressed matrix reaches ||b - A_H x|| / ||b|| <= 1e-10."""
+    from frank_b200 import BLRMatrix
+    n, nb = 2048, 8
+    rng = np.random.default_rng(2)
+    x, _ = fo.morton_sort(rng.random((dim, n)), 10)
+    M = BLRMatrix(n, nb, eps=1e-6, precision="mixed")
+    M.build_kernel("laplace", x, 1e-8)
+    M.getrf()
+    b = rng.standard_normal((n, 4))
+    xs, it, res = M.refine(b, tol=1e-10, maxit=30)
+    assert res <= 1e-10
+    r = b - M.matvec(xs)
+    assert np.max(np.linalg.norm(r, axis=0) / np.linalg.norm(b, axis=0)) <= 1e-10
+    # same answer as the plain FP64 path
+    P = BLRMatrix(n, nb, eps=1e-8, precision="fp64")
+    P.build_kernel("laplace", x, 1e-8)
+    P.getrf()
+    xp, itp, resp = P.refine(b, tol=1e-10, maxit=30)
+    assert np.linalg.norm(xs - xp) / np.linalg.norm(xp) <= 1e-8
