@@ -1,0 +1,334 @@
+"""Benchmark: BLR-LU factor + solve time to a 1e-10 residual, mixed vs plain FP64.
+
+Workload (the headline configuration): Laplace-3D kernel 1/(r + 1e-3) on
+N = 32768 uniform points in the unit cube (numpy PCG64 seed 2), Morton
+ordered (morton_index.cpp rule), BLR with 64 x 64 blocks of 512, weak
+admissibility, A_H compressed on the device to eps = 1e-8, 4 right-hand
+sides b ~ N(0, 1) (seed 3), target max_j ||b_j - A_H x_j|| / ||b_j|| <= 1e-10.
+
+One step = getrf (the FP32 factor at tolerance 1e-6 for "mixed", the FP64
+factor at 1e-8 for "fp64") + iterative refinement against the FP64 A_H to
+1e-10.  `value` is the mixed arm's time per step (seconds, device time by CUDA
+events, max over ranks), with the FP64 arm reported beside it.  Inputs
+(A_H: GBs) are larger than L2 and the working copy is reset from A_H at the
+start of every getrf.
+
+`--impl reference` times the CPU oracle (the restatement of FRANK's
+algorithm on scipy's OpenBLAS, all host cores) on a bounded sample of the
+same workload (the leading 8 x 8 blocks, N = 4096) and scales the time to
+the full workload by the ratio of algorithmic FLOPs.
+
+Multi-GPU: replicas only -- each rank factors and solves its own system
+(weak scaling), timings are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BLR-LU factor+solve time to 1e-10 residual: mixed vs plain FP64, 1 B200"
+CFG = dict(n=32768, nb=64, dim=3, eps=1e-8, mixed_eps=1e-6, nrhs=4, tol=1e-10, kernel="laplace",
+           point_seed=2, rhs_seed=3, morton_level=10)
+
+
+def make_points(n, dim, seed, level):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    x = rng.random((dim, n))
+    # Morton order (operations/misc/morton_index.cpp:36-98): pad the bounding
+    # box by 0.5, interleave `level` bits per axis, stable sort by box number.
+    bmin = x.min(axis=1) - 0.5
+    bsize = float((x.max(axis=1) - x.min(axis=1)).max()) + 1.0
+    ix = (((x - bmin[:, None]) / bsize) * (1 << level)).astype(np.int64)
+    code = np.zeros(n, dtype=np.int64)
+    for lev in range(level):
+        for d in range(dim):
+            code += (ix[d] & 1) << (dim * lev + d)
+            ix[d] >>= 1
+    return x[:, np.argsort(code, kind="stable")].copy()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (read-only query)."""
+
+    def __init__(self, gpu):
+        self.f = tempfile.NamedTemporaryFile(prefix="clk", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.f.name):
+            parts = [t.strip() for t in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1])); mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_gemm_peak(torch):
+    """Measured cuBLAS FP64 GEMM throughput (TFLOP/s), the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from frank_b200 import BLRMatrix
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    c = CFG
+    x = make_points(c["n"], c["dim"], c["point_seed"] + rank, c["morton_level"])
+    rng = np.random.default_rng(c["rhs_seed"] + rank)
+    b_host = np.asfortranarray(rng.standard_normal((c["n"], c["nrhs"])))
+    b_dev = torch.from_numpy(b_host.T.copy()).to("cuda")          # (nrhs, n) row-major == column-major n x nrhs
+    x_dev = torch.zeros_like(b_dev)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    arms = {}
+    for prec, feps in (("mixed", c["mixed_eps"]), ("fp64", c["eps"])):
+        M = BLRMatrix(c["n"], c["nb"], eps=feps, precision=prec)
+        M.build_kernel(c["kernel"], x, c["eps"])
+        torch.cuda.synchronize()
+
+        def step():
+            M.getrf(stream=stream)
+            it, res = M.refine_device(b_dev.data_ptr(), x_dev.data_ptr(), c["nrhs"], tol=c["tol"], maxit=60,
+                                      stream=stream)
+            return it, res
+
+        for _ in range(args.warmup):
+            step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = Clocks(dev) if (rank == 0 and prec == "mixed") else None
+        times, its, ress, kt = [], [], [], []
+        for _ in range(args.steps):
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            it, res = step()
+            e.record()
+            e.synchronize()
+            times.append(s.elapsed_time(e) / 1e3)
+            its.append(it); ress.append(res)
+            kt.append(M.kernel_times())
+        torch.cuda.synchronize()
+        clocks = clk.stop() if clk else None
+        if world > 1:
+            dist.barrier()
+        # end to end through the host-buffer API (H2D of b and D2H of x inside)
+        e2e = []
+        for _ in range(max(1, min(args.steps, 2))):
+            t0 = time.perf_counter()
+            M.getrf()
+            xs, it_h, res_h = M.refine(b_host, tol=c["tol"], maxit=60)
+            e2e.append(time.perf_counter() - t0)
+        st = M.stats()
+        ranks = [M.rank(i, j, 1) for i in range(c["nb"]) for j in range(c["nb"]) if i != j]
+        arms[prec] = dict(times=times, its=its, res=ress, kt=kt, e2e=e2e, clocks=clocks, stats=st,
+                          mean_rank=float(np.mean(ranks)), max_rank=int(max(ranks)))
+        M.close()
+        torch.cuda.synchronize()
+
+    peak64 = fp64_gemm_peak(torch)
+    # max over ranks of the per-step times
+    def agg(v):
+        t = torch.tensor(v, dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.cpu().tolist()
+
+    for prec in arms:
+        arms[prec]["times"] = agg(arms[prec]["times"])
+        arms[prec]["e2e"] = agg(arms[prec]["e2e"])
+    return arms, peak64
+
+
+def run_cpu_sample(threads=None):
+    """The oracle on the leading 8 x 8 blocks (N = 4096) of the workload.
+    Returns (seconds for factor + solve, algorithmic FLOPs, sample description)."""
+    import numpy as np
+    import oracle.frank_oracle as fo
+    c = CFG
+    x = make_points(c["n"], c["dim"], c["point_seed"], c["morton_level"])
+    ns, nbs = 4096, 8
+    xs = x[:, :ns].copy()
+    A = fo.build_hierarchical(fo.laplacend, xs, ns, ns // nbs, nbs, eps=c["eps"])
+    rng = np.random.default_rng(c["rhs_seed"])
+    b = rng.standard_normal((ns, c["nrhs"]))
+    fo.LRA_MODE["mode"] = "rounded_addition"
+    flops = [0.0]
+    orig = fo.rounded_addition
+
+    def counted(Ac, Bc):
+        kc, p, q = Ac.S.shape[1], Bc.U.shape[1], Bc.S.shape[1]
+        m, n = Ac.U.shape[0], Ac.V.shape[1]
+        orig(Ac, Bc)
+        s = min(kc + q, m, n)
+        r = Ac.rank
+        flops[0] += (2 * m * kc * kc + 2 * m * p * q + 4 * m * s * s - 4 / 3 * s ** 3 + 4 * n * s * s
+                     - 4 / 3 * s ** 3 + 24 * s ** 3 + 2 * m * s * r + 2 * n * s * r)
+    fo.rounded_addition = counted
+    try:
+        t0 = time.perf_counter()
+        L, U = fo.getrf(A)
+        fo.solve(L, U, b)
+        t = time.perf_counter() - t0
+    finally:
+        fo.rounded_addition = orig
+    return t, flops[0], "oracle BLR-LU (rounded_addition, scipy OpenBLAS) on the leading 8x8 blocks (N=4096) of the workload"
+
+
+def bench_reference(args, rank, world):
+    """--impl reference: rank 0 times the CPU oracle on the sample and scales
+    the time to the full workload by algorithmic FLOPs (FULL_WORKLOAD_FLOPS,
+    the recompression FLOPs the FP64 GPU run counts at eps = 1e-8 with the
+    same per-update formula).  Other ranks exit without work."""
+    if rank != 0:
+        return
+    import numpy as np
+    cores = os.cpu_count()
+    samples = []
+    for _ in range(min(args.warmup, 1)):
+        run_cpu_sample()
+    for _ in range(max(1, args.steps)):
+        t, fl, desc = run_cpu_sample()
+        samples.append((t, fl))
+    t = statistics.median([s[0] for s in samples])
+    fl = samples[0][1]
+    scale = FULL_WORKLOAD_FLOPS / fl if fl > 0 else float("nan")
+    val = t * scale
+    line = {"metric": METRIC, "value": val, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "blr-lu laplace3d N=32768 b=512 eps=1e-8 4rhs tol=1e-10",
+                       "parallelism": "replicas"},
+            "impl": "reference",
+            "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                             "sample": desc + "; %.2f s measured, scaled x%.1f by algorithmic FLOPs" % (t, scale)},
+            "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# Algorithmic FLOPs of the full workload's recompressions, measured by the GPU
+# run (kernel counters) at eps = 1e-8; used to scale the CPU sample.
+FULL_WORKLOAD_FLOPS = 1.46e13
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            bench_reference(args, rank, world)
+            return
+        arms, peak64 = run_ours(args, rank, world)
+        if rank != 0:
+            return
+        mx, fp = arms["mixed"], arms["fp64"]
+        t_mixed = statistics.median(mx["times"])
+        t_fp64 = statistics.median(fp["times"])
+        kt = mx["kt"][-1]
+        rec = kt["recompress"]
+        achieved = rec["flops"] / (rec["ms"] / 1e3) / 1e12 if rec["ms"] > 0 else 0.0
+        nrhs, n = CFG["nrhs"], CFG["n"]
+        line = {
+            "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "blr-lu laplace3d N=32768 b=512 eps=1e-8 4rhs tol=1e-10",
+                       "n": n, "block": n // CFG["nb"], "nrhs": nrhs, "mixed_factor_eps": CFG["mixed_eps"],
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2"},
+            "fp64": {"value": t_fp64, "unit": "s", "iters": fp["its"][-1], "residual": fp["res"][-1],
+                     "mean_rank": fp["mean_rank"], "max_rank": fp["max_rank"], "kernel_ms": fp["kt"][-1]},
+            "mixed": {"iters": mx["its"][-1], "residual": mx["res"][-1], "mean_rank": mx["mean_rank"],
+                      "max_rank": mx["max_rank"], "kernel_ms": kt},
+            "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "e2e": {"value": statistics.median(mx["e2e"]), "unit": "s", "fp64_value": statistics.median(fp["e2e"]),
+                    "h2d_bytes_per_step": n * nrhs * 8, "d2h_bytes_per_step": n * nrhs * 8},
+            "roofline": {"kernel": "k_recompress (mixed factor)", "bound": "tensor", "achieved": achieved,
+                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64 if peak64 else None,
+                         "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run", "traffic": None},
+            "gpu_launches": mx["stats"]["launches"],
+            "clocks": mx["clocks"],
+        }
+        if not args.no_cpu_baseline:
+            t, fl, desc = run_cpu_sample()
+            scale = FULL_WORKLOAD_FLOPS / fl
+            line["cpu_baseline"] = {"value": t * scale, "unit": "s", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": desc + "; %.2f s measured, scaled x%.1f by algorithmic FLOPs"
+                                    % (t, scale)}
+        print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -57,6 +57,7 @@ SIGNATURES = {
     "frank_blr_get_lowrank": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, C.c_int64, _dp, C.c_int64,
                                         _dp, C.c_int64, C.c_int]),
     "frank_blr_get_pivots": (C.c_int, [_vp, C.c_int, _ip]),
+    "frank_blr_set_lra": (C.c_int, [_vp, C.c_char_p, C.c_double]),
     "frank_blr_getrf": (C.c_int, [_vp, _vp]),
     "frank_blr_solve": (C.c_int, [_vp, _dp, C.c_int64, C.c_int, _vp]),
     "frank_blr_solve_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int, _vp]),
@@ -68,6 +69,7 @@ SIGNATURES = {
                                           C.c_double, C.c_int, _ip, _dp, _vp]),
     "frank_blr_solve_transpose_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int, _vp]),
     "frank_blr_stats": (C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p]),
+    "frank_blr_kernel_times": (C.c_int, [_vp, _dp, _dp]),
 }
 
 _lib = None

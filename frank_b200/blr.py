@@ -149,6 +149,11 @@ class BLRMatrix:
         return p
 
     # -- the path -----------------------------------------------------------
+    def set_lra(self, name: str, core_scale: float = 0.1):
+        """FRANK_LRA: "rounded_addition" (core SVD, the reference algorithm) or
+        "rounded_addition_rrqr" (truncated_geqp3 + rq of the core, default)."""
+        check(lib().frank_blr_set_lra(self._h, name.encode(), float(core_scale)), "frank_blr_set_lra")
+
     def getrf(self, stream: Optional[int] = None, allow=()):
         return check(lib().frank_blr_getrf(self._h, stream), "frank_blr_getrf", allow)
 
@@ -194,6 +199,14 @@ class BLRMatrix:
                                             float(tol), int(maxit), C.byref(it), C.byref(res), stream),
               "frank_blr_refine_device")
         return it.value, res.value
+
+    def kernel_times(self) -> dict:
+        """Per-class device time (ms) and algorithmic FLOPs of the last getrf."""
+        ms = np.zeros(4)
+        fl = np.zeros(4)
+        check(lib().frank_blr_kernel_times(self._h, _dptr(ms), _dptr(fl)), "frank_blr_kernel_times")
+        names = ("getrf", "panel", "dense_update", "recompress")
+        return {n: {"ms": float(ms[i]), "flops": float(fl[i])} for i, n in enumerate(names)}
 
     def stats(self) -> dict:
         v = [C.c_int64() for _ in range(4)]

@@ -60,6 +60,8 @@ struct frank_blr {
   double *getrf_scratch = nullptr, *dscratch = nullptr, *rscratch = nullptr;
   int64_t dstride = 0, rstride = 0;
   int grid_dense = 0, grid_recomp = 0, smax = 0;
+  int core_method = CORE_RRQR;
+  double core_scale = 0.1;
   // solve / matvec temporaries (nrhs <= 8 per pass)
   void* z = nullptr;         // n x 8 (T)
   void* stmp = nullptr;      // bmax x 8 (T)
@@ -74,8 +76,14 @@ struct frank_blr {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;
-  int64_t launches = 0;
+  int64_t launches = 0;        // kernels in the factorization graph
+  int64_t solve_launches = 0;  // kernels issued by solve / matvec / refine since the last getrf
   int err_h[ERR_SLOTS] = {0};
+  unsigned long long* flops = nullptr;
+  unsigned long long flops_h[FLOP_SLOTS] = {0};
+  // timing events recorded inside the captured graph: [step][class][begin,end]
+  std::vector<cudaEvent_t> ev;
+  double class_ms[FLOP_SLOTS] = {0};
 };
 
 namespace {
@@ -107,7 +115,7 @@ FactorWs<T> factor_ws(frank_blr* p) {
   w.getrf_scratch = p->getrf_scratch;
   w.dscratch = p->dscratch; w.dscratch_stride = p->dstride;
   w.rscratch = p->rscratch; w.rscratch_stride = p->rstride;
-  w.err = p->err; w.fixed_rank = p->fixed_rank; w.eps = p->eps;
+  w.err = p->err; w.flops = p->flops; w.fixed_rank = p->fixed_rank; w.eps = p->eps;
   return w;
 }
 
@@ -120,6 +128,8 @@ int check_block(const frank_blr* p, int i, int j) {
 }
 
 // Enqueue all launches of one factorization on stream s.
+cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * FLOP_SLOTS + cls) * 2 + end]; }
+
 template <typename T>
 int enqueue_factor(frank_blr* p, cudaStream_t s) {
   BlrView<double> H = h_view(p);
@@ -129,23 +139,47 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
   k_reset<T><<<p->nb * p->nb, 256, 0, s>>>(H, W);
   ++launches;
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
   for (int i = 0; i < p->nb; ++i) {
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_GETRF, 0), s));
     k_getrf<T><<<1, GETRF_THREADS, 0, s>>>(W, ws, i);
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_GETRF, 1), s));
     ++launches;
     const int m = p->nb - i - 1;
     if (m == 0) break;
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_PANEL, 0), s));
     k_panel<T><<<2 * m, PANEL_THREADS, 0, s>>>(W, ws, i);
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_PANEL, 1), s));
     ++launches;
     const int mm = m * m;
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_DENSE, 0), s));
     k_update_dense<T><<<std::min(mm, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_DENSE, 1), s));
     ++launches;
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_RECOMP, 0), s));
     if (p->nlr > 0) {
-      k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, 0, s>>>(W, ws, i, p->smax);
+      k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
+          W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale);
       ++launches;
     }
+    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_RECOMP, 1), s));
   }
   CUDA_TRY(cudaGetLastError());
   p->launches = launches;
+  return FRANK_OK;
+}
+
+// Per-class device time of the last factorization from the graph's events.
+int collect_times(frank_blr* p) {
+  for (int c = 0; c < FLOP_SLOTS; ++c) p->class_ms[c] = 0.0;
+  for (int i = 0; i < p->nb; ++i)
+    for (int c = 0; c < FLOP_SLOTS; ++c) {
+      if (i == p->nb - 1 && c != FLOP_GETRF) continue;
+      float ms = 0.f;
+      cudaError_t e = cudaEventElapsedTime(&ms, ev_at(p, i, c, 0), ev_at(p, i, c, 1));
+      if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("event timing: ") + cudaGetErrorString(e));
+      p->class_ms[c] += ms;
+    }
   return FRANK_OK;
 }
 
@@ -165,8 +199,14 @@ int run_factor(frank_blr* p, cudaStream_t s) {
   }
   CUDA_TRY(cudaGraphLaunch(p->graph_exec, s));
   CUDA_TRY(cudaMemcpyAsync(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(p->flops_h, p->flops, FLOP_SLOTS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   p->factored = true;
+  p->solve_launches = 0;
+  {
+    int rc = collect_times(p);
+    if (rc) return rc;
+  }
   if (p->err_h[ERR_SINGULAR_STEP] != 0) {
     char buf[128];
     snprintf(buf, sizeof buf, "zero pivot in the leaf getrf of diagonal block %d", p->err_h[ERR_SINGULAR_STEP] - 1);
@@ -187,6 +227,7 @@ int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cud
   T* sct = static_cast<T*>(p->sctmp);
   const size_t shm = (size_t)p->kcap * nrhs * sizeof(double);
   const int nb = p->nb;
+  p->solve_launches += 4 * nb - 2;
   if (!transpose) {
     for (int i = 0; i < nb; ++i) {
       k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 0, tmp);
@@ -223,6 +264,7 @@ int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool tra
       if (rc) return rc;
     } else {
       float* z = static_cast<float*>(p->z);
+      p->solve_launches += 2;
       k_cast_copy<float, double><<<grid_for(p->n * nr), 256, 0, s>>>(b, ldb, z, p->n, p->n, nr);
       int rc = enqueue_solve<float>(p, z, p->n, nr, transpose, s);
       if (rc) return rc;
@@ -239,6 +281,7 @@ int matvec_device_impl(frank_blr* p, const double* x, int64_t ldx, double* y, in
   for (int c0 = 0; c0 < nrhs; c0 += 8) {
     const int nr = std::min(8, nrhs - c0);
     const size_t shm = 2 * (size_t)p->kcap * nr * sizeof(double);
+    p->solve_launches += 2;
     k_matvec_blocks<<<dim3(p->nb, p->nb), MV_THREADS, shm, s>>>(H, x + c0 * ldx, ldx, nr, p->part);
     k_matvec_reduce<<<p->nb, 256, 0, s>>>(H, p->part, nr, bres ? bres + c0 * ldb : nullptr, ldb, y + c0 * ldy, ldy);
   }
@@ -251,6 +294,7 @@ int colnorms(frank_blr* p, const double* v, int64_t ldv, int nrhs, std::vector<d
   out.assign(nrhs, 0.0);
   for (int c0 = 0; c0 < nrhs; c0 += 8) {
     const int nr = std::min(8, nrhs - c0);
+    ++p->solve_launches;
     k_colnorm2<<<p->nrm_blocks, 256, 0, s>>>(v + c0 * ldv, p->n, ldv, nr, p->nrm);
     CUDA_TRY(cudaMemcpyAsync(p->nrm_h, p->nrm, sizeof(double) * p->nrm_blocks * nr, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
@@ -282,6 +326,7 @@ int refine_device_impl(frank_blr* p, const double* b, int64_t ldb, double* x, in
     for (int h = 0; h < nrhs; ++h) res = std::max(res, rn[h] / (bn[h] > 0.0 ? bn[h] : 1.0));
     if (res <= tol || it >= maxit) break;
     if ((rc = solve_device_impl(p, r, p->n, nrhs, false, s))) return rc;
+    ++p->solve_launches;
     k_axpy_cast<double><<<grid_for(p->n * nrhs), 256, 0, s>>>(r, p->n, x, ldx, p->n, nrhs);
     ++it;
   }
@@ -300,6 +345,9 @@ void free_plan(frank_blr* p) {
                   p->Wd, p->Wu, p->Ws, p->Wv, p->perm, p->ipiv, p->err, p->Linv, p->Uinv, p->WL, p->WU,
                   p->getrf_scratch, p->dscratch, p->rscratch, p->z, p->stmp, p->sctmp, p->part, p->vtmp, p->nrm};
   for (void* q : ptrs) if (q) cudaFree(q);
+  if (p->flops) cudaFree(p->flops);
+  for (cudaEvent_t e : p->ev) if (e) cudaEventDestroy(e);
+  if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
   if (p->nrm_h) cudaFreeHost(p->nrm_h);
   delete p;
 }
@@ -389,7 +437,7 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   const RecompLayout L = recomp_layout(p->bmax, p->smax);
   p->rstride = L.total;
   p->dstride = 2 * bm * bm;
-  p->grid_recomp = std::max(1, std::min(nb * nb, 2 * p->sm_count));
+  p->grid_recomp = std::max(1, std::min(nb * nb, p->sm_count));
   p->grid_dense = std::max(1, std::min(nb * nb, 2 * p->sm_count));
   p->nrm_blocks = 256;
 #define ALLOC(ptr, cnt)                                                                   \
@@ -417,6 +465,7 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   ALLOC(p->perm, nb * bm);
   ALLOC(p->ipiv, nb * bm);
   ALLOC(p->err, ERR_SLOTS);
+  ALLOC(p->flops, FLOP_SLOTS);
   ALLOC(t, nb * bm * bm * ts); p->Linv = t;
   ALLOC(t, nb * bm * bm * ts); p->Uinv = t;
   ALLOC(t, nb * bm * bm * ts); p->WL = t;
@@ -435,6 +484,9 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
     free_plan(p);
     return fail(FRANK_ERR_CUDA, "cudaMallocHost");
   }
+  p->ev.assign((size_t)nb * FLOP_SLOTS * 2, nullptr);
+  for (auto& e : p->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { free_plan(p); return fail(FRANK_ERR_CUDA, "cudaEventCreate"); }
   std::vector<int> zeros(nb * nb, 0);
   if (cudaMemcpy(p->d_off, p->off_h.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(p->d_dslot, p->dslot_h.data(), sizeof(int) * nb * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -450,6 +502,8 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   cudaFuncSetAttribute(k_matvec_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
   cudaFuncSetAttribute(k_solve_scatter<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
   cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  cudaFuncSetAttribute(k_recompress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
+  cudaFuncSetAttribute(k_recompress<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   *out = p;
   return FRANK_OK;
 }
@@ -637,6 +691,19 @@ int frank_blr_get_pivots(const frank_blr* p, int i, int* ipiv) {
   return FRANK_OK;
 }
 
+int frank_blr_set_lra(frank_blr* p, const char* name, double core_scale) {
+  if (!p || !name) return fail(FRANK_ERR_INVALID, "null argument");
+  const std::string n(name);
+  if (n == "rounded_addition") p->core_method = CORE_SVD;
+  else if (n == "rounded_addition_rrqr") p->core_method = CORE_RRQR;
+  else return fail(FRANK_ERR_UNSUPPORTED, "unknown FRANK_LRA value: " + n);
+  p->core_scale = core_scale > 0.0 ? core_scale : 0.1;
+  if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
+  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  p->factored = false;
+  return FRANK_OK;
+}
+
 int frank_blr_getrf(frank_blr* p, void* stream) {
   if (!p) return fail(FRANK_ERR_INVALID, "null plan");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -743,10 +810,19 @@ int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int6
   return rc;
 }
 
+int frank_blr_kernel_times(const frank_blr* p, double* ms, double* flops) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  for (int c = 0; c < FLOP_SLOTS; ++c) {
+    if (ms) ms[c] = p->class_ms[c];
+    if (flops) flops[c] = (double)p->flops_h[c];
+  }
+  return FRANK_OK;
+}
+
 int frank_blr_stats(const frank_blr* p, int64_t* launches, int64_t* recompressions, int64_t* max_rank_seen,
                     int64_t* rank_overflows) {
   if (!p) return fail(FRANK_ERR_INVALID, "null plan");
-  if (launches) *launches = p->launches;
+  if (launches) *launches = p->launches + p->solve_launches;
   if (recompressions) *recompressions = p->err_h[ERR_RECOMP];
   if (max_rank_seen) *max_rank_seen = p->err_h[ERR_MAX_RANK];
   if (rank_overflows) *rank_overflows = p->err_h[ERR_RANK_OVERFLOW];

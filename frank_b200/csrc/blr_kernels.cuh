@@ -47,9 +47,26 @@ struct FactorWs {
   double* rscratch;       // recompression scratch, per CTA slot
   int64_t rscratch_stride;
   int* err;
+  unsigned long long* flops;  // [FLOP_SLOTS]
   int fixed_rank;
   double eps;
 };
+
+// Algorithmic FLOPs of one rounded LowRank addition as the reference issues it
+// (gemm.cpp:253-272 then addition.cpp:93-127), counted with the LAWN 41
+// operation counts: the inner product S_A V_A U_B S_B, U_C S_C and U_B S_B,
+// geqrf + orgqr of Uc (m x s), gerqf + orgrq of VcT (s x n), the core gemm,
+// dgesvd of the s x s core (22 s^3) and the two basis gemms.
+FRANK_HD double rounded_addition_flops(double m, double n, double bi, double kc, double p, double q, double r) {
+  const double s = fmin(kc + q, fmin(m, n));
+  double f = 2.0 * p * p * bi + 2.0 * bi * q * q + 2.0 * p * bi * q;   // core of the product
+  f += 2.0 * m * kc * kc + 2.0 * m * p * q;                               // U_C S_C, U_B S_B
+  f += 4.0 * m * s * s - 4.0 / 3.0 * s * s * s;                           // geqrf + orgqr
+  f += 4.0 * n * s * s - 4.0 / 3.0 * s * s * s;                           // gerqf + orgrq
+  f += 2.0 * s * s * s + 22.0 * s * s * s;                                // Ru RvT, gesvd
+  f += 2.0 * m * s * r + 2.0 * n * s * r;                                 // new U, V
+  return f;
+}
 
 // ---------------------------------------------------------------------------
 // Reset the working copy from A_H (FP64) -- only the used parts are copied.
@@ -169,6 +186,7 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
                                       Wm + (jb + jn) + (int64_t)(jb + jn) * b, b, gsm);
   }
   if (threadIdx.x == 0) {
+    atomicAdd(ws.flops + FLOP_GETRF, (unsigned long long)(4.0 / 3.0 * (double)b * b * b));
     if (first_zero >= 0) atomicCAS(ws.err + ERR_SINGULAR_STEP, 0, i + 1);
     // permutation from the interchanges: (P B)[r] = B[perm[r]]
     for (int r = 0; r < b; ++r) perm[r] = r;
@@ -311,6 +329,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel(BlrView<T> A, FactorWs<
   const T* Li = ws.Linv + (int64_t)i * ld * ld;
   const T* Ui = ws.Uinv + (int64_t)i * ld * ld;
   const int* perm = ws.perm + (int64_t)i * ld;
+  if (threadIdx.x == 0) {
+    const int blk = (t < m) ? (i + 1 + t) * A.nb + i : i * A.nb + (i + 1 + (t - m));
+    const double kk = A.lslot[blk] >= 0 ? A.rank[blk] : A.bs(t < m ? i + 1 + t : i + 1 + (t - m));
+    atomicAdd(ws.flops + FLOP_PANEL, (unsigned long long)((double)bi * bi * kk));
+  }
   if (t < m) {
     const int ic = i + 1 + t;
     T* tmp = ws.WL + (int64_t)ic * ld * ld;
@@ -437,6 +460,9 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
     const int bc = A.bs(ic), bk = A.bs(k);
     T* C = A.dense(ic, k);
     UpdOps<T> o = update_operands(A, ws, i, ic, k);
+    if (threadIdx.x == 0)
+      atomicAdd(ws.flops + FLOP_DENSE, (unsigned long long)(2.0 * bc * bk * o.q + 2.0 * bc * o.p * o.q +
+                                                            2.0 * bi * o.p * o.q));
     if (o.left_dense && o.right_dense) {
       // C -= A(ic,i) A(i,k)
       cta_gemm<T, DUPD_THREADS>(bc, bk, bi, T(-1), o.XL, ld, false, o.YR, ld, false, T(1), C, ld, gsmt);
@@ -454,48 +480,72 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
 }
 
 // ---------------------------------------------------------------------------
-// K4: rounded addition of the update into every low-rank target of the step
-// (operations/arithmetic/addition.cpp:93-127, Bebendorf p.16):
+// K4: recompression of the update into every low-rank target of the step
+// (rounded LowRank addition, operations/arithmetic/addition.cpp:93-127,
+// Bebendorf p.16):
 //   C + W = [U_C | XL] blockdiag(S_C, T) [Vt_C | YR]^T,
-//   QR of the stacked U bases and of the stacked V bases (Householder, FP64),
-//   core M = Ru blockdiag(S_C, T) Rv^T, one-sided Jacobi SVD of M (FP64),
-//   rank by find_svd_truncation_rank (misc.cpp:133-146, quirk included) or
-//   the fixed rank, new U = Qu Um_r, V^T = Qv Vm_r, S = Sigma_r.
-// Persistent grid; each CTA owns one scratch slot (FP64) of
-// rscratch_stride doubles.
+//   blocked Householder QR of the stacked U bases and of the stacked V bases
+//   (FP64), core M = Ru blockdiag(S_C, T) Rv^T (FP64),
+//   core truncation, either
+//     RRQR: truncated column-pivoted QR of M to core_scale * eps * ||M||_F,
+//           then RQ of the kept rows, i.e. the reference's own fixed-accuracy
+//           compressor LowRank(Dense, eps) (low_rank.cpp:50-59, geqp3.cpp:71-192)
+//           applied to the core; S comes out upper triangular;
+//     SVD:  one-sided Jacobi of M with the rank of find_svd_truncation_rank
+//           (misc.cpp:133-146, quirk included) or the fixed rank; S diagonal;
+//   new U = Qu [Q_core; 0], new V^T = Qv [V_core; 0].
+// Persistent grid, one target per CTA at a time, FP64 scratch slot per CTA.
+// The core lives in shared memory when it fits (RECOMP_SMEM_CORE doubles).
 // ---------------------------------------------------------------------------
 constexpr int RECOMP_THREADS = 512;
+constexpr int RECOMP_SMEM_BYTES = 200 * 1024;           // dynamic shared memory
+constexpr int RECOMP_GSM = 2 * 16 * 64;                 // cta_gemm tiles (doubles)
+constexpr int RECOMP_REGION = RECOMP_SMEM_BYTES / 8 - RECOMP_GSM;  // doubles for panels / core
+enum CoreMethod { CORE_RRQR = 0, CORE_SVD = 1 };
 
 struct RecompLayout {
-  int64_t ash, bsh, tm, mtmp, mm, m0, sig, ord, xo, yo, tau_u, tau_v, total;
+  int64_t ash, bsh, tm, rc, rv, mtmp, mglob, m0, xo, yo, tfu, tfv, w, tau_u, tau_v, tau_c, tau2, cn, pn, jp, ji, total;
 };
 
 FRANK_HD RecompLayout recomp_layout(int bmax, int smax) {
-  // smax: max stacked width (kcap + max(p, q))
   RecompLayout L;
   int64_t o = 0;
   auto take = [&](int64_t n) { int64_t r = o; o += (n + 31) & ~int64_t(31); return r; };
   const int mu = smax < bmax ? smax : bmax;
+  const int64_t np = (smax + QRB - 1) / QRB;
   L.ash = take((int64_t)bmax * smax);
   L.bsh = take((int64_t)bmax * smax);
   L.tm = take((int64_t)bmax * bmax);
+  L.rc = take((int64_t)mu * smax);
+  L.rv = take((int64_t)mu * smax);
   L.mtmp = take((int64_t)mu * smax);
-  L.mm = take((int64_t)mu * mu);
+  L.mglob = take((int64_t)mu * mu);
   L.m0 = take((int64_t)mu * mu);
-  L.sig = take(mu);
-  L.ord = take(mu);
   L.xo = take((int64_t)bmax * mu);
   L.yo = take((int64_t)bmax * mu);
+  L.tfu = take(np * QRB * QRB);
+  L.tfv = take(np * QRB * QRB);
+  L.w = take((int64_t)QRB * (smax > bmax ? smax : bmax));
   L.tau_u = take(smax);
   L.tau_v = take(smax);
+  L.tau_c = take(mu);
+  L.tau2 = take(mu);
+  L.cn = take(mu);
+  L.pn = take(mu);
+  L.jp = take(mu);
+  L.ji = take(mu);
   L.total = o;
   return L;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax) {
-  __shared__ double gsm[2 * 16 * 64];
+__global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
+                                                               int core_method, double core_scale) {
+  extern __shared__ double dsm[];
+  double* gsm = dsm;
+  double* region = dsm + RECOMP_GSM;
   __shared__ double red[32];
+  __shared__ int redi[32];
   __shared__ int flag;
   __shared__ int s_rank;
   const int m = A.nb - i - 1;
@@ -506,15 +556,26 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
   double* Ash = base + L.ash;
   double* Bsh = base + L.bsh;
   double* Tm = base + L.tm;
+  double* Rc = base + L.rc;
+  double* Rv = base + L.rv;
   double* Mtmp = base + L.mtmp;
-  double* Mm = base + L.mm;
+  double* Mg = base + L.mglob;
   double* M0 = base + L.m0;
-  double* sig = base + L.sig;
-  int* ord = reinterpret_cast<int*>(base + L.ord);
   double* Xo = base + L.xo;
   double* Yo = base + L.yo;
+  double* Tfu = base + L.tfu;
+  double* Tfv = base + L.tfv;
+  double* Wq = base + L.w;
   double* tau_u = base + L.tau_u;
   double* tau_v = base + L.tau_v;
+  double* tau_c = base + L.tau_c;
+  double* tau2 = base + L.tau2;
+  double* cnorm = base + L.cn;
+  double* pnorm = base + L.pn;
+  int* jpvt = reinterpret_cast<int*>(base + L.jp);
+  int* jinv = reinterpret_cast<int*>(base + L.ji);
+  double* smP = region;
+  double* smT = region + (int64_t)A.bmax * QRB;
   for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
     const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
     if (!A.is_lr(ic, k)) continue;
@@ -533,10 +594,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     // stacked bases in FP64
     for (int64_t e = threadIdx.x; e < (int64_t)bc * su; e += blockDim.x) {
       const int r = e % bc, c = e / bc;
-      double v;
-      if (c < kc) v = double(Uc[r + (int64_t)c * ld]);
-      else v = double(o.XL[r + (int64_t)(c - kc) * ld]);
-      Ash[r + (int64_t)c * bc] = v;
+      Ash[r + (int64_t)c * bc] = (c < kc) ? double(Uc[r + (int64_t)c * ld]) : double(o.XL[r + (int64_t)(c - kc) * ld]);
     }
     for (int64_t e = threadIdx.x; e < (int64_t)bk * sv; e += blockDim.x) {
       const int r = e % bk, c = e / bk;
@@ -547,115 +605,171 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       Bsh[r + (int64_t)c * bk] = v;
     }
     form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
-    cta_householder_qr(bc, su, Ash, bc, tau_u, red);
-    cta_householder_qr(bk, sv, Bsh, bk, tau_v, red);
+    cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
+    cta_qr_blocked<RECOMP_THREADS>(bk, sv, Bsh, bk, tau_v, Tfv, Wq, smP, smT, gsm, red);
     const int mu = min(bc, su), mv = min(bk, sv);
-    // Mtmp (mu x sv) = Ru * blockdiag(S_C, T)
-    for (int64_t e = threadIdx.x; e < (int64_t)mu * sv; e += blockDim.x) {
+    // clean upper-trapezoidal R factors
+    for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
       const int r = e % mu, c = e / mu;
-      double s = 0.0;
-      if (c < kc) {
-        for (int t = r; t < kc; ++t) s += Ash[r + (int64_t)t * bc] * double(Sc[t + (int64_t)c * A.kcap]);
-      } else {
-        const int cc = c - kc;
-        for (int t = max(r, kc); t < su; ++t) s += Ash[r + (int64_t)t * bc] * Tm[(t - kc) + (int64_t)cc * o.p];
+      Rc[e] = (r <= c) ? Ash[r + (int64_t)c * bc] : 0.0;
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)mv * sv; e += blockDim.x) {
+      const int r = e % mv, c = e / mv;
+      Rv[e] = (r <= c) ? Bsh[r + (int64_t)c * bk] : 0.0;
+    }
+    __syncthreads();
+    // Mtmp (mu x sv) = [Rc[:, :kc] S_C | Rc[:, kc:] T]
+    cta_gemm<double, RECOMP_THREADS>(mu, kc, kc, 1.0, Rc, mu, false, Sc, A.kcap, false, 0.0, Mtmp, mu, gsm);
+    cta_gemm<double, RECOMP_THREADS>(mu, o.q, o.p, 1.0, Rc + (int64_t)kc * mu, mu, false, Tm, o.p, false, 0.0,
+                                     Mtmp + (int64_t)kc * mu, mu, gsm);
+    // core M (mu x mv) = Mtmp Rv^T, in shared memory if it fits
+    const bool in_smem = (int64_t)mu * mv + 4 * (int64_t)mv + 2 * mu <= RECOMP_REGION;
+    double* Mm = in_smem ? region : Mg;
+    cta_gemm<double, RECOMP_THREADS>(mu, mv, sv, 1.0, Mtmp, mu, false, Rv, mv, true, 0.0, Mm, mu, gsm);
+    int r = 0;
+    if (core_method == CORE_RRQR && ws.fixed_rank == 0) {
+      double f = 0.0;
+      for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) f += Mm[e] * Mm[e];
+      f = block_sum(f, red);
+      double* cn = in_smem ? region + (int64_t)mu * mv : cnorm;
+      double* pn = in_smem ? cn + mv : pnorm;
+      double* tc = in_smem ? pn + mv : tau_c;
+      r = cta_truncated_geqp3(mu, mv, Mm, mu, core_scale * ws.eps * sqrt(f), A.kcap, tc, cn, pn, jpvt, red, redi);
+      if (r == 0) {
+        // zero core: rank-1 zero block (geqp3.cpp:97-102)
+        if (threadIdx.x == 0) { atomicMax(ws.err + ERR_MAX_RANK, 1); atomicAdd(ws.err + ERR_RECOMP, 1); }
+        for (int64_t e = threadIdx.x; e < (int64_t)bc; e += blockDim.x) Uc[e] = T(e == 0 ? 1.0 : 0.0);
+        for (int64_t e = threadIdx.x; e < (int64_t)bk; e += blockDim.x) Vc[e] = T(e == 0 ? 1.0 : 0.0);
+        if (threadIdx.x == 0) { Sc[0] = T(0); A.rank[blk] = 1; }
+        __syncthreads();
+        continue;
       }
-      Mtmp[r + (int64_t)c * mu] = s;
-    }
-    __syncthreads();
-    // M (mu x mv) = Mtmp * Rv^T ; Rv (mv x sv) upper trapezoid in Bsh
-    for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) {
-      const int r = e % mu, c = e / mu;
-      double s = 0.0;
-      for (int t = c; t < sv; ++t) s += Mtmp[r + (int64_t)t * mu] * Bsh[c + (int64_t)t * bk];
-      Mm[r + (int64_t)c * mu] = s;
-      M0[r + (int64_t)c * mu] = s;
-    }
-    __syncthreads();
-    const int sweeps = cta_jacobi_columns(mu, mv, Mm, mu, 60, &flag);
-    if (sweeps < 0 && threadIdx.x == 0) atomicAdd(ws.err + ERR_JACOBI, 1);
-    // column norms
-    for (int c = threadIdx.x >> 5; c < mv; c += blockDim.x >> 5) {
-      double s = 0.0;
-      for (int r = threadIdx.x & 31; r < mu; r += 32) s += Mm[r + (int64_t)c * mu] * Mm[r + (int64_t)c * mu];
-      s = warp_sum(s);
-      if ((threadIdx.x & 31) == 0) sig[c] = sqrt(s);
-    }
-    __syncthreads();
-    // descending order: rank of each column = #(larger) + #(equal with smaller index)
-    for (int c = threadIdx.x; c < mv; c += blockDim.x) {
-      const double v = sig[c];
-      int pos = 0;
-      for (int d = 0; d < mv; ++d) {
-        const double w = sig[d];
-        pos += (w > v) || (w == v && d < c);
+      if (threadIdx.x == 0) {
+        if (r >= A.kcap && r < min(mu, mv)) atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1);
+        atomicMax(ws.err + ERR_MAX_RANK, r);
+        atomicAdd(ws.err + ERR_RECOMP, 1);
       }
-      ord[pos] = c;
-    }
-    __syncthreads();
-    const int nsv = min(mu, mv);
-    if (threadIdx.x == 0) {
-      int r;
-      if (ws.fixed_rank > 0) {
-        r = min(ws.fixed_rank, nsv);
-      } else {
-        double fro = 0.0;
-        for (int j = 0; j < nsv; ++j) { const double v = sig[ord[j]]; fro += v * v; }
-        const double thr = ws.eps * sqrt(fro);
-        r = 0;
-        double err;
-        do {
-          ++r;
-          err = 0.0;
-          if (r < nsv) {
-            const double v = sig[ord[r]];
-            for (int j = r; j < nsv; ++j) err += v * v;
-          }
-        } while (r < nsv && sqrt(err) > thr);
+      // Xo (bc x r) = [Q_core; 0]
+      for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+        const int rr = e % bc, c = e / bc;
+        Xo[e] = (rr == c) ? 1.0 : 0.0;
       }
-      if (r > A.kcap) { atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1); r = A.kcap; }
-      atomicMax(ws.err + ERR_MAX_RANK, r);
-      atomicAdd(ws.err + ERR_RECOMP, 1);
-      s_rank = r;
+      __syncthreads();
+      cta_apply_q(mu, r, Mm, mu, tc, r, Xo, (int64_t)bc);
+      // X2 (mv x r) = R_perm^T J, R_perm[:, jpvt[c']] = R[:, c']
+      for (int c = threadIdx.x; c < mv; c += blockDim.x) jinv[jpvt[c]] = c;
+      __syncthreads();
+      double* X2 = Mtmp;
+      for (int64_t e = threadIdx.x; e < (int64_t)mv * r; e += blockDim.x) {
+        const int c = e % mv, a = e / mv;
+        const int row = r - 1 - a, src = jinv[c];
+        X2[e] = (row <= src) ? Mm[row + (int64_t)src * mu] : 0.0;
+      }
+      __syncthreads();
+      cta_householder_qr(mv, r, X2, mv, tau2, red);
+      // S = J Rt^T J (upper triangular)
+      for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
+        const int a = e % r, c = e / r;
+        const int ra = r - 1 - c, ca = r - 1 - a;
+        Sc[a + (int64_t)c * A.kcap] = T((ra <= ca) ? X2[ra + (int64_t)ca * mv] : 0.0);
+      }
+      // Qt (mv x r) explicit into Rc, then Yo[:, a] = [Qt[:, r-1-a]; 0]
+      double* Qt = Rc;
+      for (int64_t e = threadIdx.x; e < (int64_t)mv * r; e += blockDim.x) {
+        const int rr = e % mv, c = e / mv;
+        Qt[e] = (rr == c) ? 1.0 : 0.0;
+      }
+      __syncthreads();
+      cta_apply_q(mv, r, X2, mv, tau2, r, Qt, (int64_t)mv);
+      for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+        const int rr = e % bk, a = e / bk;
+        Yo[e] = (rr < mv) ? Qt[rr + (int64_t)(r - 1 - a) * mv] : 0.0;
+      }
+      __syncthreads();
+    } else {
+      // SVD core: keep a copy for the V side, Jacobi in place
+      for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) M0[e] = Mm[e];
+      __syncthreads();
+      const int sweeps = cta_jacobi_columns(mu, mv, Mm, mu, 60, &flag);
+      if (sweeps < 0 && threadIdx.x == 0) atomicAdd(ws.err + ERR_JACOBI, 1);
+      double* sig = cnorm;
+      int* ord = jpvt;
+      for (int c = threadIdx.x >> 5; c < mv; c += blockDim.x >> 5) {
+        double sacc = 0.0;
+        for (int rr = threadIdx.x & 31; rr < mu; rr += 32) sacc += Mm[rr + (int64_t)c * mu] * Mm[rr + (int64_t)c * mu];
+        sacc = warp_sum(sacc);
+        if ((threadIdx.x & 31) == 0) sig[c] = sqrt(sacc);
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < mv; c += blockDim.x) {
+        const double v = sig[c];
+        int pos = 0;
+        for (int d = 0; d < mv; ++d) {
+          const double w = sig[d];
+          pos += (w > v) || (w == v && d < c);
+        }
+        ord[pos] = c;
+      }
+      __syncthreads();
+      const int nsv = min(mu, mv);
+      if (threadIdx.x == 0) {
+        int rr;
+        if (ws.fixed_rank > 0) {
+          rr = min(ws.fixed_rank, nsv);
+        } else {
+          double fro = 0.0;
+          for (int j = 0; j < nsv; ++j) { const double v = sig[ord[j]]; fro += v * v; }
+          const double thr = ws.eps * sqrt(fro);
+          rr = 0;
+          double err;
+          do {
+            ++rr;
+            err = 0.0;
+            if (rr < nsv) {
+              const double v = sig[ord[rr]];
+              for (int j = rr; j < nsv; ++j) err += v * v;
+            }
+          } while (rr < nsv && sqrt(err) > thr);
+        }
+        if (rr > A.kcap) { atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1); rr = A.kcap; }
+        atomicMax(ws.err + ERR_MAX_RANK, rr);
+        atomicAdd(ws.err + ERR_RECOMP, 1);
+        s_rank = rr;
+      }
+      __syncthreads();
+      r = s_rank;
+      for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+        const int rr = e % bc, c = e / bc;
+        const int src = ord[c];
+        const double sv_ = sig[src];
+        Xo[e] = (rr < mu && sv_ > 0.0) ? Mm[rr + (int64_t)src * mu] / sv_ : 0.0;
+      }
+      __syncthreads();
+      // Yo (bk x r): rows < mv = M0^T Um / sigma
+      cta_gemm<double, RECOMP_THREADS>(mv, r, mu, 1.0, M0, mu, true, Xo, bc, false, 0.0, Yo, bk, gsm);
+      for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+        const int rr = e % bk, c = e / bk;
+        const double sv_ = sig[ord[c]];
+        Yo[e] = (rr < mv && sv_ > 0.0) ? Yo[e] / sv_ : 0.0;
+      }
+      for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
+        const int rr = e % r, c = e / r;
+        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? sig[ord[c]] : 0.0);
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    const int r = s_rank;
-    // Um_r (mu x r) normalized columns -> Xo (bc x r, rows >= mu zero)
+    if (threadIdx.x == 0)
+      atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r));
+    // U = Qu Xo ; Vt = Qv Yo  (blocked WY application)
+    cta_apply_q_blocked<RECOMP_THREADS>(bc, mu, Ash, bc, Tfu, r, Xo, (int64_t)bc, Wq, smP, smT, gsm);
+    cta_apply_q_blocked<RECOMP_THREADS>(bk, mv, Bsh, bk, Tfv, r, Yo, (int64_t)bk, Wq, smP, smT, gsm);
     for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
       const int rr = e % bc, c = e / bc;
-      const int src = ord[c];
-      const double sv_ = sig[src];
-      double v = 0.0;
-      if (rr < mu && sv_ > 0.0) v = Mm[rr + (int64_t)src * mu] / sv_;
-      Xo[rr + (int64_t)c * bc] = v;
-    }
-    __syncthreads();
-    // Vm_r (mv x r) = M0^T Um_r / sigma -> Yo (bk x r, rows >= mv zero)
-    for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
-      const int rr = e % bk, c = e / bk;
-      double v = 0.0;
-      const double sv_ = sig[ord[c]];
-      if (rr < mv && sv_ > 0.0) {
-        for (int t = 0; t < mu; ++t) v += M0[t + (int64_t)rr * mu] * Xo[t + (int64_t)c * bc];
-        v /= sv_;
-      }
-      Yo[rr + (int64_t)c * bk] = v;
-    }
-    __syncthreads();
-    // U = Qu Xo ; Vt = Qv Yo
-    cta_apply_q(bc, mu, Ash, bc, tau_u, r, Xo, (int64_t)bc);
-    cta_apply_q(bk, mv, Bsh, bk, tau_v, r, Yo, (int64_t)bk);
-    for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
-      const int rr = e % bc, c = e / bc;
-      Uc[rr + (int64_t)c * ld] = T(Xo[rr + (int64_t)c * bc]);
+      Uc[rr + (int64_t)c * ld] = T(Xo[e]);
     }
     for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
       const int rr = e % bk, c = e / bk;
-      Vc[rr + (int64_t)c * ld] = T(Yo[rr + (int64_t)c * bk]);
-    }
-    for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
-      const int rr = e % r, c = e / r;
-      Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? sig[ord[c]] : 0.0);
+      Vc[rr + (int64_t)c * ld] = T(Yo[e]);
     }
     if (threadIdx.x == 0) A.rank[blk] = r;
     __syncthreads();

@@ -24,6 +24,10 @@ enum ErrSlot {
   ERR_SLOTS = 8
 };
 
+// Algorithmic FLOP counters (device unsigned long long array of the plan),
+// one per kernel class of the factorization.
+enum FlopSlot { FLOP_GETRF = 0, FLOP_PANEL = 1, FLOP_DENSE = 2, FLOP_RECOMP = 3, FLOP_SLOTS = 4 };
+
 FRANK_D double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -288,6 +292,242 @@ FRANK_D int cta_jacobi_columns(int m, int n, double* G, int64_t ldg, int max_swe
     if (!rotated) return sweep + 1;
   }
   return -1;
+}
+
+}  // namespace frank
+
+namespace frank {
+
+// ---------------------------------------------------------------------------
+// Blocked Householder QR in FP64 (LAPACK dgeqrf with dgeqr2 panels, dlarft
+// forward/columnwise T factors and dlarfb trailing updates), column-major A
+// (m x n, lda) in global memory.  Panels of QRB columns are factored in shared
+// memory; the trailing matrix is updated as A -= V (T^T (V^T A)) by two
+// CTA GEMMs.  On return A holds R and the reflectors, tau[min(m,n)], and the
+// T factor of panel p at Tf + p*QRB*QRB (column-major, ld QRB).
+// Shared memory: smP (m*QRB doubles), smT (QRB*QRB), gsm (cta_gemm tiles),
+// red (32).  Global scratch W (QRB x n doubles).
+// ---------------------------------------------------------------------------
+constexpr int QRB = 32;
+
+// Gram-based T factor of the panel V (mr x jn, unit lower trapezoid in smV).
+FRANK_D void cta_larft(int mr, int jn, const double* smV, const double* tau, double* smT) {
+  // G = V^T V (upper part), then T column by column (dlarft recurrence).
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int e = wid; e < jn * jn; e += nw) {
+    const int i = e % jn, j = e / jn;
+    if (i >= j) continue;
+    double s = 0.0;
+    for (int r = lane; r < mr; r += 32) s += smV[r + (int64_t)i * mr] * smV[r + (int64_t)j * mr];
+    s = warp_sum(s);
+    if (lane == 0) smT[i + j * QRB] = s;  // G(i,j), i<j, temporarily in T's upper part
+  }
+  __syncthreads();
+  // T column by column (dlarft recurrence), one warp: lane i owns row i.
+  // G(l, j) (l < j) sits in T's upper part until column j is produced.
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    for (int j = 0; j < jn; ++j) {
+      double s = 0.0;
+      if (i < j)
+        for (int l = i; l < j; ++l) s += smT[i + l * QRB] * smT[l + j * QRB];
+      __syncwarp();
+      if (i < j) smT[i + j * QRB] = -tau[j] * s;
+      if (i == j) smT[j + j * QRB] = tau[j];
+      if (i > j) smT[i + j * QRB] = 0.0;
+      __syncwarp();
+    }
+    for (int j = jn; j < QRB; ++j) smT[i + j * QRB] = 0.0;
+  }
+  __syncthreads();
+}
+
+// Load the panel's reflectors from A (rows j0.., cols j0..j0+jn) into smV as a
+// clean unit-lower-trapezoidal matrix (mr x jn, ld mr).
+FRANK_D void cta_load_v(int mr, int jn, const double* Ap, int64_t lda, double* smV) {
+  for (int e = threadIdx.x; e < mr * jn; e += blockDim.x) {
+    const int r = e % mr, c = e / mr;
+    smV[e] = (r > c) ? Ap[r + (int64_t)c * lda] : (r == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+}
+
+template <int NT>
+FRANK_D void cta_qr_blocked(int m, int n, double* A, int64_t lda, double* tau, double* Tf, double* W,
+                            double* smP, double* smT, double* gsm, double* red) {
+  const int kmin = m < n ? m : n;
+  for (int j0 = 0; j0 < kmin; j0 += QRB) {
+    const int jn = min(QRB, kmin - j0);
+    const int mr = m - j0;
+    double* Ap = A + j0 + (int64_t)j0 * lda;
+    for (int e = threadIdx.x; e < mr * jn; e += blockDim.x) {
+      const int r = e % mr, c = e / mr;
+      smP[e] = Ap[r + (int64_t)c * lda];
+    }
+    __syncthreads();
+    cta_householder_qr(mr, jn, smP, mr, tau + j0, red);
+    for (int e = threadIdx.x; e < mr * jn; e += blockDim.x) {
+      const int r = e % mr, c = e / mr;
+      Ap[r + (int64_t)c * lda] = smP[e];
+      smP[e] = (r > c) ? smP[e] : (r == c ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    cta_larft(mr, jn, smP, tau + j0, smT);
+    double* Tp = Tf + (int64_t)(j0 / QRB) * QRB * QRB;
+    for (int e = threadIdx.x; e < QRB * QRB; e += blockDim.x) Tp[e] = smT[e];
+    const int nc = n - j0 - jn;
+    if (nc > 0) {
+      double* At = A + j0 + (int64_t)(j0 + jn) * lda;
+      // W = V^T At (jn x nc)
+      cta_gemm<double, NT>(jn, nc, mr, 1.0, smP, mr, true, At, lda, false, 0.0, W, QRB, gsm);
+      // W = T^T W (T upper triangular): column per thread
+      for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        double w[QRB];
+        for (int i = 0; i < jn; ++i) w[i] = W[i + (int64_t)c * QRB];
+        for (int i = jn - 1; i >= 0; --i) {
+          double s = 0.0;
+          for (int l = 0; l <= i; ++l) s += smT[l + i * QRB] * w[l];
+          W[i + (int64_t)c * QRB] = s;
+        }
+      }
+      __syncthreads();
+      // At -= V W
+      cta_gemm<double, NT>(mr, nc, jn, -1.0, smP, mr, false, W, QRB, false, 1.0, At, lda, gsm);
+    }
+  }
+  __syncthreads();
+}
+
+// X (m x r, ldx, FP64) := Q X with Q from cta_qr_blocked (k = min(m, ncols)
+// reflectors).  Panels applied last to first: X -= V (T (V^T X)).
+template <int NT>
+FRANK_D void cta_apply_q_blocked(int m, int k, const double* A, int64_t lda, const double* Tf, int r,
+                                 double* X, int64_t ldx, double* W, double* smP, double* smT, double* gsm) {
+  if (k <= 0 || r <= 0) { __syncthreads(); return; }
+  const int np = (k + QRB - 1) / QRB;
+  for (int p = np - 1; p >= 0; --p) {
+    const int j0 = p * QRB;
+    const int jn = min(QRB, k - j0);
+    const int mr = m - j0;
+    cta_load_v(mr, jn, A + j0 + (int64_t)j0 * lda, lda, smP);
+    for (int e = threadIdx.x; e < QRB * QRB; e += blockDim.x) smT[e] = Tf[(int64_t)p * QRB * QRB + e];
+    __syncthreads();
+    double* Xp = X + j0;
+    cta_gemm<double, NT>(jn, r, mr, 1.0, smP, mr, true, Xp, ldx, false, 0.0, W, QRB, gsm);
+    for (int c = threadIdx.x; c < r; c += blockDim.x) {
+      double w[QRB];
+      for (int i = 0; i < jn; ++i) w[i] = W[i + (int64_t)c * QRB];
+      for (int i = 0; i < jn; ++i) {
+        double s = 0.0;
+        for (int l = i; l < jn; ++l) s += smT[i + l * QRB] * w[l];
+        W[i + (int64_t)c * QRB] = s;
+      }
+    }
+    __syncthreads();
+    cta_gemm<double, NT>(mr, r, jn, -1.0, smP, mr, false, W, QRB, false, 1.0, Xp, ldx, gsm);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Truncated column-pivoted Householder QR (restating
+// operations/LAPACK/geqp3.cpp:71-192: pivot = first column of largest
+// down-dated norm, dlarfg reflector, LAWN 176 norm down-dating, stop when the
+// largest remaining norm <= thr or after maxr steps).  In place on A (m x n,
+// lda, FP64; shared or global memory).  Returns the rank r; jpvt[c] is the
+// original column at pivoted position c.  cnorm/partial: n doubles each.
+// ---------------------------------------------------------------------------
+FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr, int maxr, double* tau,
+                                double* cnorm, double* partial, int* jpvt, double* red, int* redi) {
+  const double dlamch_e = 1.1102230246251565e-16;
+  const double tol3z = sqrt(dlamch_e);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int mind = min(min(m, n), maxr);
+  for (int c = wid; c < n; c += nw) {
+    double s = 0.0;
+    for (int r = lane; r < m; r += 32) s += A[r + (int64_t)c * lda] * A[r + (int64_t)c * lda];
+    s = warp_sum(s);
+    if (lane == 0) { cnorm[c] = sqrt(s); partial[c] = sqrt(s); jpvt[c] = c; }
+  }
+  __syncthreads();
+  double maxc;
+  {
+    double best = -1.0; int bi = -1;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+    block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+  }
+  int r = 0;
+  while (r < mind && maxc > thr) {
+    double best = -1.0; int bi = -1;
+    for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+    double dummy;
+    const int kp = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &dummy);
+    if (kp != r) {
+      for (int e = threadIdx.x; e < m; e += blockDim.x) {
+        const double a = A[e + (int64_t)r * lda];
+        A[e + (int64_t)r * lda] = A[e + (int64_t)kp * lda];
+        A[e + (int64_t)kp * lda] = a;
+      }
+      if (threadIdx.x == 0) {
+        double a = cnorm[r]; cnorm[r] = cnorm[kp]; cnorm[kp] = a;
+        a = partial[r]; partial[r] = partial[kp]; partial[kp] = a;
+        int q = jpvt[r]; jpvt[r] = jpvt[kp]; jpvt[kp] = q;
+      }
+    }
+    __syncthreads();
+    double* col = A + (int64_t)r * lda;
+    double s = 0.0;
+    for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) s += col[e] * col[e];
+    const double xn2 = block_sum(s, red);
+    const double alpha = col[r];
+    double tt = 0.0, beta = alpha;
+    if (xn2 > 0.0) {
+      const double nrm = sqrt(alpha * alpha + xn2);
+      beta = alpha >= 0.0 ? -nrm : nrm;
+      tt = (beta - alpha) / beta;
+      const double scal = 1.0 / (alpha - beta);
+      for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) col[e] *= scal;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { col[r] = beta; tau[r] = tt; }
+    __syncthreads();
+    if (r < min(m, n) - 1 && tt != 0.0) {
+      for (int c = r + 1 + wid; c < n; c += nw) {
+        double* cc = A + (int64_t)c * lda;
+        double w = (lane == 0) ? cc[r] : 0.0;
+        for (int e = r + 1 + lane; e < m; e += 32) w += col[e] * cc[e];
+        w = warp_sum(w) * tt;
+        if (lane == 0) cc[r] -= w;
+        for (int e = r + 1 + lane; e < m; e += 32) cc[e] -= w * col[e];
+      }
+    }
+    __syncthreads();
+    for (int c = r + 1 + wid; c < n; c += nw) {
+      if (cnorm[c] != 0.0) {
+        double temp = fabs(A[r + (int64_t)c * lda] / cnorm[c]);
+        temp = fmax(0.0, (1.0 - temp) * (1.0 + temp));
+        const double ratio = cnorm[c] / partial[c];
+        const double temp2 = temp * ratio * ratio;
+        if (temp2 > tol3z) {
+          if (lane == 0) cnorm[c] = cnorm[c] * sqrt(temp);
+        } else {
+          double s2 = 0.0;
+          if (r < m - 1)
+            for (int e = r + 1 + lane; e < m; e += 32) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
+          s2 = warp_sum(s2);
+          if (lane == 0) { cnorm[c] = (r < m - 1) ? sqrt(s2) : 0.0; partial[c] = cnorm[c]; }
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    ++r;
+    best = -1.0; bi = -1;
+    for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+    block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+    if (r >= n) maxc = 0.0;
+  }
+  __syncthreads();
+  return r;
 }
 
 }  // namespace frank

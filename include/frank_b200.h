@@ -127,6 +127,17 @@ int frank_blr_get_lowrank(const frank_blr* plan, int which, int i, int j,
 /* LAPACK-style 1-based pivot rows of the diagonal block i (after getrf). */
 int frank_blr_get_pivots(const frank_blr* plan, int i, int* ipiv);
 
+/* Select the LowRank recompression of the factorization, like FRANK's
+ * setGlobalValue("FRANK_LRA", name) (util/global_key_value.cpp:10-22, read at
+ * operations/arithmetic/addition.cpp:194-201):
+ *   "rounded_addition"       core SVD (one-sided Jacobi, FP64) truncated by
+ *                            find_svd_truncation_rank -- the reference algorithm;
+ *   "rounded_addition_rrqr"  (default) the reference's fixed-accuracy compressor
+ *                            truncated_geqp3 + rq applied to the same core, with
+ *                            tolerance core_scale * eps (core_scale <= 0: 0.1).
+ * Fixed-rank plans always use the core SVD. */
+int frank_blr_set_lra(frank_blr* plan, const char* name, double core_scale);
+
 /* Right-looking block LU in place.  Replaces getrf(Hierarchical&)
  * (operations/LAPACK/getrf.cpp:40-65) with its leaf getrf (getrf.cpp:67-84,
  * here with partial pivoting applied), trsm (operations/BLAS/trsm.cpp:92-115),
@@ -163,10 +174,18 @@ int frank_blr_refine_device(frank_blr* plan, const double* d_b, int64_t ldb, dou
  * the adjoint of solve(A, b) (no reference counterpart; python/FRANK adjoint). */
 int frank_blr_solve_transpose_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
 
-/* Counters of the last getrf: kernel launches issued, and the sum over all
- * recompressions of (rank before, rank after) for reporting. */
+/* Counters of the last getrf: kernels launched by it plus those of every
+ * solve / matvec / refine since, recompressions performed, the largest
+ * recompressed rank and the number of ranks clamped at max_rank. */
 int frank_blr_stats(const frank_blr* plan, int64_t* launches, int64_t* recompressions,
                     int64_t* max_rank_seen, int64_t* rank_overflows);
+
+/* Device time (ms, CUDA events recorded around each launch inside the
+ * factorization graph) and algorithmic FLOPs of the last getrf, per kernel
+ * class: [0] leaf getrf + inverses, [1] panel trsm, [2] dense-target updates,
+ * [3] LowRank recompression.  The FLOPs count the reference's call sequence
+ * with the LAWN 41 operation counts (no reference counterpart; reporting). */
+int frank_blr_kernel_times(const frank_blr* plan, double* ms, double* flops);
 
 #ifdef __cplusplus
 }

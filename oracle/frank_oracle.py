@@ -588,6 +588,33 @@ def rounded_addition(A: LowRank, B: LowRank) -> None:
     A.V = gemm(RRV[:r, :], QvT)
 
 
+def rounded_addition_rrqr(A: LowRank, B: LowRank) -> None:
+    """Variant used by this engine's GPU path (NOT a reference algorithm):
+    identical stacking to rounded_addition, but the core M = Ru RvT is
+    truncated with the reference's own fixed-accuracy compressor
+    (truncated_geqp3 + rq, low_rank.cpp:50-59) instead of dgesvd +
+    find_svd_truncation_rank.  Used only to bound the deviation in tests."""
+    if A.eps == 0:
+        rounded_addition(A, B)
+        return
+    ka, kb = A.S.shape[1], B.S.shape[1]
+    m = A.U.shape[0]
+    Uc = np.zeros((m, ka + kb))
+    Uc[:, :ka] = gemm(A.U, A.S)
+    Uc[:, ka:] = gemm(B.U, B.S)
+    s = min(Uc.shape)
+    Qu, Ru = qr_dense(Uc, q_cols=s, r_rows=s)
+    VcT = np.vstack([A.V, B.V])
+    RvT, QvT = rq_dense(VcT)
+    M = gemm(Ru, RvT)
+    Qm, Rm = truncated_geqp3(M, A.eps)
+    Sm, Vm = rq_dense(Rm)
+    A.rank = Qm.shape[1]
+    A.S = Sm
+    A.U = gemm(Qu, Qm)
+    A.V = gemm(Vm, QvT)
+
+
 def fast_rounded_addition(A: LowRank, B: LowRank) -> None:
     """operations/arithmetic/addition.cpp:133-189 (Bebendorf p.17); falls back
     to rounded_addition for fixed accuracy."""
@@ -639,6 +666,8 @@ def lr_add(A: LowRank, B: LowRank) -> None:
     mode = LRA_MODE["mode"]
     if mode == "naive":
         naive_addition(A, B)
+    elif mode == "rounded_addition_rrqr":
+        rounded_addition_rrqr(A, B)
     elif mode == "rounded_addition":
         rounded_addition(A, B)
     else:
