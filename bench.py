@@ -6,7 +6,7 @@ ordered (morton_index.cpp rule), BLR with 64 x 64 blocks of 512, weak
 admissibility, A_H compressed on the device to eps = 1e-8, 4 right-hand
 sides b ~ N(0, 1) (seed 3), target max_j ||b_j - A_H x_j|| / ||b_j|| <= 1e-10.
 
-One step = getrf (the FP32 factor at tolerance 1e-6 for "mixed", the FP64
+One step = getrf (the FP32 factor at tolerance 1e-3 for "mixed", the FP64
 factor at 1e-8 for "fp64") + iterative refinement against the FP64 A_H to
 1e-10.  `value` is the mixed arm's time per step (seconds, device time by CUDA
 events, max over ranks), with the FP64 arm reported beside it.  Inputs
@@ -36,7 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "BLR-LU factor+solve time to 1e-10 residual: mixed vs plain FP64, 1 B200"
-CFG = dict(n=32768, nb=64, dim=3, eps=1e-8, mixed_eps=1e-6, nrhs=4, tol=1e-10, kernel="laplace",
+CFG = dict(n=32768, nb=64, dim=3, eps=1e-8, mixed_eps=1e-3, nrhs=4, tol=1e-10, kernel="laplace",
            point_seed=2, rhs_seed=3, morton_level=10)
 
 
@@ -265,14 +265,36 @@ def bench_reference(args, rank, world):
 FULL_WORKLOAD_FLOPS = 1.46e13
 
 
+def profile_case(name):
+    """Small single-GPU cases for ncu captures (`--profile-case`): build the
+    plan, run one getrf, print the per-class kernel times.
+      n8192: Laplace-3D N=8192, 16 x 16 blocks of 512, A_H eps 1e-8, mixed
+             factor at 1e-6 (the recompression profile case)."""
+    import torch
+    from frank_b200 import BLRMatrix
+    if name != "n8192":
+        raise SystemExit("unknown profile case " + name)
+    x = make_points(8192, 3, 2, 10)
+    M = BLRMatrix(8192, 16, eps=1e-6, precision="mixed")
+    M.build_kernel("laplace", x, 1e-8)
+    M.getrf()
+    torch.cuda.synchronize()
+    print(json.dumps(M.kernel_times()))
+    M.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-case", default=None, help="run a small ncu case instead of the benchmark")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1:

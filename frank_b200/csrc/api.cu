@@ -141,28 +141,28 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
   for (int i = 0; i < p->nb; ++i) {
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_GETRF, 0), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_GETRF, 0), s, cudaEventRecordExternal));
     k_getrf<T><<<1, GETRF_THREADS, 0, s>>>(W, ws, i);
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_GETRF, 1), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_GETRF, 1), s, cudaEventRecordExternal));
     ++launches;
     const int m = p->nb - i - 1;
     if (m == 0) break;
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_PANEL, 0), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
     k_panel<T><<<2 * m, PANEL_THREADS, 0, s>>>(W, ws, i);
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_PANEL, 1), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 1), s, cudaEventRecordExternal));
     ++launches;
     const int mm = m * m;
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_DENSE, 0), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s, cudaEventRecordExternal));
     k_update_dense<T><<<std::min(mm, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_DENSE, 1), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
     ++launches;
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_RECOMP, 0), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 0), s, cudaEventRecordExternal));
     if (p->nlr > 0) {
       k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
           W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale);
       ++launches;
     }
-    CUDA_TRY(cudaEventRecord(ev_at(p, i, FLOP_RECOMP, 1), s));
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 1), s, cudaEventRecordExternal));
   }
   CUDA_TRY(cudaGetLastError());
   p->launches = launches;
