@@ -70,6 +70,8 @@ SIGNATURES = {
     "frank_blr_solve_transpose_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int, _vp]),
     "frank_blr_stats": (C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p]),
     "frank_blr_kernel_times": (C.c_int, [_vp, _dp, _dp]),
+    "frank_getrf_dense_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
+                                            _vp]),
 }
 
 _lib = None

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -830,3 +831,117 @@ int frank_blr_stats(const frank_blr* p, int64_t* launches, int64_t* recompressio
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free dense getrf (frank_getrf_dense_noalloc).
+//
+// For callers that cannot call cudaMalloc (inside an allocator callback, on an
+// out-of-memory recovery path, under a pool that forbids growth).  All device
+// scratch comes from the file-scope array below: the block copy D, the FP64
+// work matrix of k_getrf, the explicit inverses k_getrf also forms, the pivot
+// and permutation vectors, and the small geometry / status words.  Nothing in
+// this section changes the plan-based paths above.
+// ===========================================================================
+namespace {
+
+constexpr int NOALLOC_N = FRANK_NOALLOC_MAX_N;
+constexpr size_t NA_MAT = (size_t)NOALLOC_N * NOALLOC_N * sizeof(double);  // 512 KB
+constexpr size_t NA_D = 0;
+constexpr size_t NA_W = NA_D + NA_MAT;
+constexpr size_t NA_LINV = NA_W + NA_MAT;
+constexpr size_t NA_UINV = NA_LINV + NA_MAT;
+constexpr size_t NA_PERM = NA_UINV + NA_MAT;
+constexpr size_t NA_IPIV = NA_PERM + NOALLOC_N * sizeof(int);
+constexpr size_t NA_GEOM = NA_IPIV + NOALLOC_N * sizeof(int);            // off[2], dslot, lslot, rank
+constexpr size_t NA_ERR = NA_GEOM + 8 * sizeof(int);                    // ERR_SLOTS ints
+constexpr size_t NA_FLOPS = NA_ERR + ERR_SLOTS * sizeof(int);           // FLOP_SLOTS ull
+constexpr size_t NA_BYTES = NA_FLOPS + FLOP_SLOTS * sizeof(unsigned long long);
+
+// The scratch: fixed size, resident on every GPU that loads the library.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+// Geometry of a one-block plan, pivots back to 1-based; device code names the
+// array directly.
+__global__ void k_noalloc_prepare(int n) {
+  int* g = reinterpret_cast<int*>(g_noalloc_scratch + NA_GEOM);
+  g[0] = 0; g[1] = n;   // off[0..1]
+  g[2] = 0;             // dslot[0]
+  g[3] = -1;            // lslot[0]
+  g[4] = 0;             // rank[0]
+  int* e = reinterpret_cast<int*>(g_noalloc_scratch + NA_ERR);
+  for (int k = 0; k < ERR_SLOTS; ++k) e[k] = 0;
+  unsigned long long* f = reinterpret_cast<unsigned long long*>(g_noalloc_scratch + NA_FLOPS);
+  for (int k = 0; k < FLOP_SLOTS; ++k) f[k] = 0ull;
+}
+
+__global__ void k_noalloc_pivots(int n, int* out) {
+  const int* ip = reinterpret_cast<const int*>(g_noalloc_scratch + NA_IPIV);
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) out[r] = ip[r] + 1;
+}
+
+// Device address of the scratch, looked up once per device (the host-side
+// name of a __device__ array is not a device address).
+constexpr int NA_MAX_DEVICES = 64;
+unsigned char* g_noalloc_addr[NA_MAX_DEVICES] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+int noalloc_setup(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(FRANK_ERR_UNSUPPORTED, "device index beyond the set-up table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(FRANK_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(ptr);
+  }
+  *out = g_noalloc_addr[dev];
+  return FRANK_OK;
+}
+
+}  // namespace
+
+extern "C" int frank_getrf_dense_noalloc(const double* d_a, int64_t lda, int n, double* d_lu, int64_t ldlu,
+                                         int* d_ipiv, void* stream) {
+  if (n < 1 || n > NOALLOC_N) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "frank_getrf_dense_noalloc: n = %d outside 1..%d (the size of its fixed scratch)", n,
+             NOALLOC_N);
+    return fail(FRANK_ERR_UNSUPPORTED, buf);
+  }
+  if (!d_a || !d_lu || !d_ipiv || lda < n || ldlu < n) return fail(FRANK_ERR_INVALID, "bad noalloc getrf arguments");
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  unsigned char* base = nullptr;
+  int rc = noalloc_setup(dev, &base);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int* geom = reinterpret_cast<int*>(base + NA_GEOM);
+  BlrView<double> A;
+  A.nb = 1; A.bmax = n; A.kcap = 0;
+  A.off = geom; A.dslot = geom + 2; A.lslot = geom + 3; A.rank = geom + 4;
+  A.D = reinterpret_cast<double*>(base + NA_D);
+  A.U = A.S = A.Vt = nullptr;
+  FactorWs<double> ws{};
+  ws.perm = reinterpret_cast<int*>(base + NA_PERM);
+  ws.ipiv = reinterpret_cast<int*>(base + NA_IPIV);
+  ws.Linv = reinterpret_cast<double*>(base + NA_LINV);
+  ws.Uinv = reinterpret_cast<double*>(base + NA_UINV);
+  ws.getrf_scratch = reinterpret_cast<double*>(base + NA_W);
+  ws.err = reinterpret_cast<int*>(base + NA_ERR);
+  ws.flops = reinterpret_cast<unsigned long long*>(base + NA_FLOPS);
+  k_noalloc_prepare<<<1, 1, 0, s>>>(n);
+  CUDA_TRY(cudaMemcpy2DAsync(A.D, n * sizeof(double), d_a, lda * sizeof(double), n * sizeof(double), n,
+                             cudaMemcpyDeviceToDevice, s));
+  k_getrf<double><<<1, GETRF_THREADS, 0, s>>>(A, ws, 0);
+  CUDA_TRY(cudaMemcpy2DAsync(d_lu, ldlu * sizeof(double), A.D, n * sizeof(double), n * sizeof(double), n,
+                             cudaMemcpyDeviceToDevice, s));
+  k_noalloc_pivots<<<1, 256, 0, s>>>(n, d_ipiv);
+  CUDA_TRY(cudaGetLastError());
+  int err_words[ERR_SLOTS];
+  CUDA_TRY(cudaMemcpyAsync(err_words, ws.err, sizeof(err_words), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (err_words[ERR_SINGULAR_STEP] != 0) return fail(FRANK_ERR_SINGULAR, "zero pivot in the dense block");
+  return FRANK_OK;
+}
+

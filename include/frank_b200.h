@@ -187,6 +187,35 @@ int frank_blr_stats(const frank_blr* plan, int64_t* launches, int64_t* recompres
  * with the LAWN 41 operation counts (no reference counterpart; reporting). */
 int frank_blr_kernel_times(const frank_blr* plan, double* ms, double* flops);
 
+/* Largest block order accepted by frank_getrf_dense_noalloc. */
+#define FRANK_NOALLOC_MAX_N 256
+
+/* Pivoted LU of one dense FP64 block that allocates no memory.  No
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc, e.g. code running inside a custom device-memory allocator's
+ * callback, on an out-of-memory recovery path where every byte is already
+ * committed, or in a process whose memory pool forbids new allocations.
+ * The plan-based entry points allocate device memory (the plan itself, and
+ * staging buffers in the host-buffer calls); this one uses only the fixed
+ * scratch described below and the caller's buffers.
+ *
+ * d_a: n x n input (device, column-major, lda >= n), left unchanged.
+ * d_lu: n x n output (device, column-major, ldlu >= n): the packed LU of
+ * P A (unit L below the diagonal, U on and above), the same factor as
+ * frank_blr_getrf on a one-block plan.  d_ipiv: n ints (device), 1-based
+ * LAPACK-style pivots.  n must be 1..FRANK_NOALLOC_MAX_N, else
+ * FRANK_ERR_UNSUPPORTED; a zero pivot gives FRANK_ERR_SINGULAR.
+ *
+ * The scratch is one fixed 2 MB array in device memory (a file-scope
+ * __device__ array of the library) that every GPU loading the library holds
+ * until exit; all calls share it and it keeps the last call's contents.  The
+ * first call on a device looks up the array's device address (set-up, once
+ * per device); make that first call before any stream capture.  The call is
+ * synchronous on `stream`.  Calls that overlap on the GPU (from several host
+ * threads or streams at once) race on the shared scratch: serialise them. */
+int frank_getrf_dense_noalloc(const double* d_a, int64_t lda, int n, double* d_lu, int64_t ldlu,
+                              int* d_ipiv, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
