@@ -63,6 +63,9 @@ struct frank_blr {
   int grid_dense = 0, grid_recomp = 0, smax = 0;
   int core_method = CORE_RRQR;
   double core_scale = 0.1;
+  int grid_gram = 0;
+  double gram_tol = 1e-12;
+  bool gram = false;
   // solve / matvec temporaries (nrhs <= 8 per pass)
   void* z = nullptr;         // n x 8 (T)
   void* stmp = nullptr;      // bmax x 8 (T)
@@ -85,6 +88,10 @@ struct frank_blr {
   // timing events recorded inside the captured graph: [step][class][begin,end]
   std::vector<cudaEvent_t> ev;
   double class_ms[FLOP_SLOTS] = {0};
+  // lookahead: second capture stream and its dependency events
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> getrf_done, dense_done;
 };
 
 namespace {
@@ -129,23 +136,44 @@ int check_block(const frank_blr* p, int i, int j) {
 }
 
 // Enqueue all launches of one factorization on stream s.
+// The Gram-based recompression serves the mixed path with the RRQR core at a
+// tolerance (fixed-rank plans and the SVD core use the Householder kernel).
+bool use_gram(const frank_blr* p) {
+  return p->precision == FRANK_PREC_MIXED && p->fixed_rank == 0 && p->core_method == CORE_RRQR && p->gram;
+}
+
 cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * FLOP_SLOTS + cls) * 2 + end]; }
 
+// One factorization on stream s.  The leaf getrf of step i+1 runs on a second
+// stream (p->aux) as soon as step i's dense-target update has refreshed the
+// diagonal block (i+1, i+1), so it overlaps step i's recompressions
+// (lookahead of depth one); the panel of step i+1 waits for both.  The
+// recompression grid leaves one SM free for it.
 template <typename T>
 int enqueue_factor(frank_blr* p, cudaStream_t s) {
   BlrView<double> H = h_view(p);
   BlrView<T> W = work_view<T>(p);
   FactorWs<T> ws = factor_ws<T>(p);
+  cudaStream_t s2 = p->aux;
   int64_t launches = 0;
   k_reset<T><<<p->nb * p->nb, 256, 0, s>>>(H, W);
   ++launches;
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
+  CUDA_TRY(cudaEventRecord(p->fork, s));
+  CUDA_TRY(cudaStreamWaitEvent(s2, p->fork, 0));
+  auto getrf_on_aux = [&](int step) -> int {
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 0), s2, cudaEventRecordExternal));
+    k_getrf<T><<<1, GETRF_THREADS, 0, s2>>>(W, ws, step);
+    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 1), s2, cudaEventRecordExternal));
+    CUDA_TRY(cudaEventRecord(p->getrf_done[step], s2));
+    return FRANK_OK;
+  };
+  int rc = getrf_on_aux(0);
+  if (rc) return rc;
+  ++launches;
   for (int i = 0; i < p->nb; ++i) {
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_GETRF, 0), s, cudaEventRecordExternal));
-    k_getrf<T><<<1, GETRF_THREADS, 0, s>>>(W, ws, i);
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_GETRF, 1), s, cudaEventRecordExternal));
-    ++launches;
+    CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[i], 0));
     const int m = p->nb - i - 1;
     if (m == 0) break;
     CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
@@ -157,14 +185,32 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
     k_update_dense<T><<<std::min(mm, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
     CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
     ++launches;
+    CUDA_TRY(cudaEventRecord(p->dense_done[i], s));
+    CUDA_TRY(cudaStreamWaitEvent(s2, p->dense_done[i], 0));
+    if ((rc = getrf_on_aux(i + 1))) return rc;
+    ++launches;
     CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 0), s, cudaEventRecordExternal));
     if (p->nlr > 0) {
-      k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-          W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale);
-      ++launches;
+      if (use_gram(p)) {
+        // mixed path: Gram-based recompression of every low-rank x low-rank
+        // update; the Householder kernel takes any target with a dense operand
+        k_recompress_gram<T><<<std::min(mm, p->grid_gram), GRAM_THREADS, GRAM_SMEM_BYTES, s>>>(
+            W, ws, i, p->smax, p->core_scale, p->gram_tol);
+        ++launches;
+        if (p->dense_offdiag) {
+          k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
+              W, ws, i, p->smax, p->core_method, p->core_scale, 1);
+          ++launches;
+        }
+      } else {
+        k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
+            W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0);
+        ++launches;
+      }
     }
     CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 1), s, cudaEventRecordExternal));
   }
+  CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[p->nb - 1], 0));
   CUDA_TRY(cudaGetLastError());
   p->launches = launches;
   return FRANK_OK;
@@ -348,6 +394,10 @@ void free_plan(frank_blr* p) {
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->flops) cudaFree(p->flops);
   for (cudaEvent_t e : p->ev) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->getrf_done) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->dense_done) if (e) cudaEventDestroy(e);
+  if (p->fork) cudaEventDestroy(p->fork);
+  if (p->aux) cudaStreamDestroy(p->aux);
   if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
   if (p->nrm_h) cudaFreeHost(p->nrm_h);
   delete p;
@@ -436,9 +486,11 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   const int64_t bm = p->bmax, kc = p->kcap;
   p->smax = (int)(kc + (p->dense_offdiag ? bm : kc));
   const RecompLayout L = recomp_layout(p->bmax, p->smax);
-  p->rstride = L.total;
+  const GramLayout LG = gram_layout(p->bmax, p->smax);
+  p->rstride = std::max(L.total, LG.total);
   p->dstride = 2 * bm * bm;
-  p->grid_recomp = std::max(1, std::min(nb * nb, p->sm_count));
+  p->grid_recomp = std::max(1, std::min(nb * nb, p->sm_count - 1));
+  p->grid_gram = std::max(1, std::min(nb * nb, 2 * (p->sm_count - 1)));
   p->grid_dense = std::max(1, std::min(nb * nb, 2 * p->sm_count));
   p->nrm_blocks = 256;
 #define ALLOC(ptr, cnt)                                                                   \
@@ -471,9 +523,11 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   ALLOC(t, nb * bm * bm * ts); p->Uinv = t;
   ALLOC(t, nb * bm * bm * ts); p->WL = t;
   ALLOC(t, nb * bm * bm * ts); p->WU = t;
-  ALLOC(p->getrf_scratch, bm * bm);
+  ALLOC(p->getrf_scratch, bm * bm + 32 * bm);
   ALLOC(p->dscratch, (int64_t)p->grid_dense * p->dstride);
-  if (p->nlr > 0) ALLOC(p->rscratch, (int64_t)p->grid_recomp * p->rstride);
+  if (p->nlr > 0)
+    ALLOC(p->rscratch, (int64_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
+                           p->rstride);
   ALLOC(t, p->n * 8 * ts); p->z = t;
   ALLOC(t, bm * 8 * ts); p->stmp = t;
   ALLOC(t, (int64_t)nb * bm * 8 * ts); p->sctmp = t;
@@ -488,6 +542,19 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   p->ev.assign((size_t)nb * FLOP_SLOTS * 2, nullptr);
   for (auto& e : p->ev)
     if (cudaEventCreate(&e) != cudaSuccess) { free_plan(p); return fail(FRANK_ERR_CUDA, "cudaEventCreate"); }
+  p->getrf_done.assign(nb, nullptr);
+  p->dense_done.assign(nb, nullptr);
+  for (auto* v : {&p->getrf_done, &p->dense_done})
+    for (auto& e : *v)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+        free_plan(p);
+        return fail(FRANK_ERR_CUDA, "cudaEventCreate");
+      }
+  if (cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking) != cudaSuccess) {
+    free_plan(p);
+    return fail(FRANK_ERR_CUDA, "lookahead stream");
+  }
   std::vector<int> zeros(nb * nb, 0);
   if (cudaMemcpy(p->d_off, p->off_h.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(p->d_dslot, p->dslot_h.data(), sizeof(int) * nb * nb, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -505,6 +572,8 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
   cudaFuncSetAttribute(k_recompress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
+  cudaFuncSetAttribute(k_recompress_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, GRAM_SMEM_BYTES);
+  cudaFuncSetAttribute(k_recompress_gram<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, GRAM_SMEM_BYTES);
   *out = p;
   return FRANK_OK;
 }
@@ -695,8 +764,9 @@ int frank_blr_get_pivots(const frank_blr* p, int i, int* ipiv) {
 int frank_blr_set_lra(frank_blr* p, const char* name, double core_scale) {
   if (!p || !name) return fail(FRANK_ERR_INVALID, "null argument");
   const std::string n(name);
-  if (n == "rounded_addition") p->core_method = CORE_SVD;
-  else if (n == "rounded_addition_rrqr") p->core_method = CORE_RRQR;
+  if (n == "rounded_addition") { p->core_method = CORE_SVD; p->gram = false; }
+  else if (n == "rounded_addition_rrqr") { p->core_method = CORE_RRQR; p->gram = false; }
+  else if (n == "rounded_addition_rrqr_gram") { p->core_method = CORE_RRQR; p->gram = true; }
   else return fail(FRANK_ERR_UNSUPPORTED, "unknown FRANK_LRA value: " + n);
   p->core_scale = core_scale > 0.0 ? core_scale : 0.1;
   if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
@@ -832,6 +902,18 @@ int frank_blr_stats(const frank_blr* p, int64_t* launches, int64_t* recompressio
 
 }  // extern "C"
 
+#ifdef FRANK_PHASE_TIMING
+// Read and clear the recompression phase counters (timing builds only).
+extern "C" int frank_debug_phase_cycles(unsigned long long* cycles16, unsigned long long* count2) {
+  CUDA_TRY(cudaMemcpyFromSymbol(cycles16, g_phase_cycles, sizeof(unsigned long long) * 16));
+  CUDA_TRY(cudaMemcpyFromSymbol(count2, g_phase_count, sizeof(unsigned long long) * 2));
+  unsigned long long z[16] = {0};
+  CUDA_TRY(cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z)));
+  CUDA_TRY(cudaMemcpyToSymbol(g_phase_count, z, sizeof(unsigned long long) * 2));
+  return FRANK_OK;
+}
+#endif
+
 // ===========================================================================
 // Allocation-free dense getrf (frank_getrf_dense_noalloc).
 //
@@ -848,7 +930,7 @@ constexpr int NOALLOC_N = FRANK_NOALLOC_MAX_N;
 constexpr size_t NA_MAT = (size_t)NOALLOC_N * NOALLOC_N * sizeof(double);  // 512 KB
 constexpr size_t NA_D = 0;
 constexpr size_t NA_W = NA_D + NA_MAT;
-constexpr size_t NA_LINV = NA_W + NA_MAT;
+constexpr size_t NA_LINV = NA_W + NA_MAT + (size_t)32 * NOALLOC_N * sizeof(double);  // k_getrf work + panel
 constexpr size_t NA_UINV = NA_LINV + NA_MAT;
 constexpr size_t NA_PERM = NA_UINV + NA_MAT;
 constexpr size_t NA_IPIV = NA_PERM + NOALLOC_N * sizeof(int);

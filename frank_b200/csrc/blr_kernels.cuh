@@ -32,6 +32,26 @@ struct BlrView {
   FRANK_D T* vt(int i, int j) const { return Vt + (int64_t)lslot[i * nb + j] * bmax * kcap; }
 };
 
+// Optional per-phase cycle counters of the recompression kernels (build with
+// -DFRANK_PHASE_TIMING; off by default).  Slots: [size class][phase].
+#ifdef FRANK_PHASE_TIMING
+__device__ unsigned long long g_phase_cycles[2][8];
+__device__ unsigned long long g_phase_count[2];
+#define PHASE_BEGIN() long long _ph_t0 = clock64(); int _ph_last = 0
+#define PHASE_MARK(cls, k)                                                                  \
+  do {                                                                                      \
+    if (threadIdx.x == 0) {                                                                 \
+      const long long _t = clock64();                                                      \
+      atomicAdd(&g_phase_cycles[(cls)][(k)], (unsigned long long)(_t - _ph_t0));            \
+      _ph_t0 = _t;                                                                          \
+    }                                                                                       \
+    (void)_ph_last;                                                                         \
+  } while (0)
+#else
+#define PHASE_BEGIN() do {} while (0)
+#define PHASE_MARK(cls, k) do {} while (0)
+#endif
+
 // Per-factorization workspace (device pointers).
 template <typename T>
 struct FactorWs {
@@ -41,7 +61,7 @@ struct FactorWs {
   T* Uinv;        // [nb][bmax*bmax]: upper inverse per diagonal block
   T* WL;          // [nb][bmax*bmax]: (S V)^T of column-panel blocks, by block row
   T* WU;          // [nb][bmax*bmax]: U S of row-panel blocks, by block column
-  double* getrf_scratch;  // bmax*bmax
+  double* getrf_scratch;  // bmax*bmax + 32*bmax
   double* dscratch;       // dense-update scratch, per CTA slot
   int64_t dscratch_stride;
   double* rscratch;       // recompression scratch, per CTA slot
@@ -126,7 +146,8 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
   const int b = A.bs(i);
   const int ldA = A.bmax;
   T* Dp = A.dense(i, i);
-  double* Wm = ws.getrf_scratch;
+  double* Wm = ws.getrf_scratch;                       // b x b working matrix
+  double* Gp = Wm + (int64_t)A.bmax * A.bmax;          // 32 x bmax product panel
   int* piv = ws.ipiv + (int64_t)i * A.bmax;
   int* perm = ws.perm + (int64_t)i * A.bmax;
   T* Li = ws.Linv + (int64_t)i * A.bmax * A.bmax;
@@ -170,15 +191,30 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
       }
       __syncthreads();
     }
-    // U12 = L11^{-1} A12
-    for (int c = jb + jn + threadIdx.x; c < b; c += blockDim.x) {
-      for (int r = 1; r < jn; ++r) {
-        double s = Wm[(jb + r) + (int64_t)c * b];
-        for (int t = 0; t < r; ++t) s -= Wm[(jb + r) + (int64_t)(jb + t) * b] * Wm[(jb + t) + (int64_t)c * b];
-        Wm[(jb + r) + (int64_t)c * b] = s;
+    // U12 = L11^{-1} A12: invert the unit-lower 32x32 L11 into tri, then a
+    // CTA GEMM into the scratch panel and back.
+    const int ncr = b - jb - jn;
+    if (ncr > 0) {
+      for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
+      __syncthreads();
+      if (threadIdx.x < jn) {
+        const int c = threadIdx.x;
+        tri[c + c * 33] = 1.0;
+        for (int r = c + 1; r < jn; ++r) {
+          double s = 0.0;
+          for (int t = c; t < r; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
+          tri[r + c * 33] = -s;
+        }
       }
+      __syncthreads();
+      cta_gemm<double, GETRF_THREADS>(jn, ncr, jn, 1.0, tri, 33, false, Wm + jb + (int64_t)(jb + jn) * b, b, false,
+                                      0.0, Gp, 32, gsm);
+      for (int e = threadIdx.x; e < jn * ncr; e += blockDim.x) {
+        const int r = e % jn, c = e / jn;
+        Wm[(jb + r) + (int64_t)(jb + jn + c) * b] = Gp[r + (int64_t)c * 32];
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const int m2 = b - jb - jn;
     if (m2 > 0)
       cta_gemm<double, GETRF_THREADS>(m2, m2, jn, -1.0, Wm + (jb + jn) + (int64_t)jb * b, b, false,
@@ -201,16 +237,10 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
     Dp[r + (int64_t)c * ldA] = T(Wm[r + (int64_t)c * b]);
   }
   __syncthreads();
-  // ---- Uinv: X = U^{-1}, blocked by 32-column blocks from the left ----
-  // X[0:j, j:j+jn] = -(X[0:j,0:j] U[0:j, j:j+jn]) inv(U_jj); X_jj = inv(U_jj).
-  // Built in FP64 in the Linv/Uinv slot of T is not possible for T=float, so
-  // the FP64 result is staged in the upper triangle region of a second FP64
-  // buffer: we reuse Wm's strictly-lower part? No -- keep it simple: compute
-  // each output block column into shared memory and write it in T, reading
-  // previously written columns back from T (ok: values are rounded once).
+  // ---- Uinv = U^{-1}, by 32-column blocks from the left (dtrtri order):
+  //   X_jj = inv(U_jj);  X[0:jb, jb:jb+jn] = -(X[0:jb, 0:jb] U[0:jb, jb:jb+jn]) X_jj
   for (int jb = 0; jb < b; jb += 32) {
     const int jn = min(32, b - jb);
-    // inv(U_jj) into tri (jn x jn, ld 33)
     for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
     __syncthreads();
     if (threadIdx.x < jn) {
@@ -223,38 +253,22 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
       }
     }
     __syncthreads();
-    // zero the column block of Ui, write the diagonal block
-    for (int e = threadIdx.x; e < b * jn; e += blockDim.x) {
-      const int r = e % b, c = e / b;
-      double v = 0.0;
-      if (r >= jb && r < jb + jn) v = tri[(r - jb) + c * 33];
-      Ui[r + (int64_t)(jb + c) * ldA] = T(v);
+    if (jb > 0) {
+      // Gp (jb x jn) = X[0:jb, 0:jb] U[0:jb, jb:jb+jn]   (U read from the upper part of Wm)
+      cta_gemm<double, GETRF_THREADS>(jb, jn, jb, 1.0, Ui, ldA, false, Wm + (int64_t)jb * b, b, false, 0.0, Gp, jb,
+                                      gsm);
+      // X[0:jb, jb:jb+jn] = -Gp X_jj
+      cta_gemm<double, GETRF_THREADS>(jb, jn, jn, -1.0, Gp, jb, false, tri, 33, false, 0.0, Ui + (int64_t)jb * ldA,
+                                      ldA, gsm);
+    }
+    for (int e = threadIdx.x; e < (b - jb) * jn; e += blockDim.x) {
+      const int r = jb + e % (b - jb), c = e / (b - jb);
+      Ui[r + (int64_t)(jb + c) * ldA] = T((r < jb + jn) ? tri[(r - jb) + c * 33] : 0.0);
     }
     __syncthreads();
-    if (jb > 0) {
-      // tmp (jb x jn) = X[0:jb, 0:jb] * U[0:jb, jb:jb+jn]  -> stored in Wm's
-      // strictly-lower area is unsafe; use the Li slot as FP64-free temp is
-      // also T-typed.  So compute column by column with FP64 registers:
-      // each thread owns (row r, col c) and accumulates over t in [r, jb).
-      for (int e = threadIdx.x; e < jb * jn; e += blockDim.x) {
-        const int r = e % jb, c = e / jb;
-        double s = 0.0;
-        for (int t = r; t < jb; ++t) s += double(Ui[r + (int64_t)t * ldA]) * Wm[t + (int64_t)(jb + c) * b];
-        // multiply by inv(U_jj) later: stash s in Li (T) temporarily
-        Li[r + (int64_t)c * ldA] = T(s);
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < jb * jn; e += blockDim.x) {
-        const int r = e % jb, c = e / jb;
-        double s = 0.0;
-        for (int t = 0; t <= c; ++t) s += double(Li[r + (int64_t)t * ldA]) * tri[t + c * 33];
-        Ui[r + (int64_t)(jb + c) * ldA] = T(-s);
-      }
-      __syncthreads();
-    }
   }
-  // ---- Linv: X = L^{-1} (unit lower), blocked from the bottom ----
-  // X[j+jn:b, j:j+jn] = -(X[j+jn:b, j+jn:b] L[j+jn:b, j:j+jn]) inv(L_jj)
+  // ---- Linv = L^{-1} (unit lower), by 32-column blocks from the bottom:
+  //   X_jj = inv(L_jj);  X[jb+jn:b, jb:jb+jn] = -(X[jb+jn:b, jb+jn:b] L[jb+jn:b, jb:jb+jn]) X_jj
   const int nblk = (b + 31) / 32;
   for (int blk = nblk - 1; blk >= 0; --blk) {
     const int jb = blk * 32;
@@ -272,38 +286,17 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
     }
     __syncthreads();
     const int below = b - jb - jn;
-    // temp product into the (not yet written) upper rows [0, jb) of this
-    // column block of Li, which are zero in the final result
     if (below > 0) {
-      // product P (below x jn) = X[jb+jn:, jb+jn:] * L[jb+jn:, jb:jb+jn]
-      // stash in FP64 inside Wm's upper triangle is not allowed (U still
-      // needed? no: U is already in Dp and Ui), so use Wm's upper-right part.
-      double* tmp = Wm;  // overwrite rows 0..below-1, cols 0..jn-1 of Wm (U part no longer needed except L below)
-      // Wm's upper triangle (r < c) held U; U is consumed.  Rows 0..below-1 x
-      // cols 0..jn-1 overlap the lower part when r > c, so use a column
-      // offset that keeps us strictly in the upper triangle: cols [b-jn, b)
-      // with rows [0, below): r < below <= b - jn <= c  => r < c.  Safe.
-      for (int e = threadIdx.x; e < below * jn; e += blockDim.x) {
-        const int r = e % below, c = e / below;
-        double s = 0.0;
-        const int gr = jb + jn + r;
-        for (int t = jb + jn; t <= gr; ++t) s += double(Li[gr + (int64_t)t * ldA]) * Wm[t + (int64_t)(jb + c) * b];
-        tmp[r + (int64_t)(b - jn + c) * b] = s;
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < below * jn; e += blockDim.x) {
-        const int r = e % below, c = e / below;
-        double s = 0.0;
-        for (int t = c; t < jn; ++t) s += tmp[r + (int64_t)(b - jn + t) * b] * tri[t + c * 33];
-        Li[(jb + jn + r) + (int64_t)(jb + c) * ldA] = T(-s);
-      }
-      __syncthreads();
+      // L[jb+jn:b, jb:jb+jn] is the strictly-lower part of Wm; X[jb+jn:, jb+jn:]
+      // (already final, zero above its diagonal) is in Li.
+      cta_gemm<double, GETRF_THREADS>(below, jn, below, 1.0, Li + (jb + jn) + (int64_t)(jb + jn) * ldA, ldA, false,
+                                      Wm + (jb + jn) + (int64_t)jb * b, b, false, 0.0, Gp, below, gsm);
+      cta_gemm<double, GETRF_THREADS>(below, jn, jn, -1.0, Gp, below, false, tri, 33, false, 0.0,
+                                      Li + (jb + jn) + (int64_t)jb * ldA, ldA, gsm);
     }
     for (int e = threadIdx.x; e < (jb + jn) * jn; e += blockDim.x) {
       const int r = e % (jb + jn), c = e / (jb + jn);
-      double v = 0.0;
-      if (r >= jb) v = tri[(r - jb) + c * 33];
-      Li[r + (int64_t)(jb + c) * ldA] = T(v);
+      Li[r + (int64_t)(jb + c) * ldA] = T((r >= jb) ? tri[(r - jb) + c * 33] : 0.0);
     }
     __syncthreads();
   }
@@ -540,7 +533,8 @@ FRANK_HD RecompLayout recomp_layout(int bmax, int smax) {
 
 template <typename T>
 __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
-                                                               int core_method, double core_scale) {
+                                                               int core_method, double core_scale,
+                                                               int only_dense_operands) {
   extern __shared__ double dsm[];
   double* gsm = dsm;
   double* region = dsm + RECOMP_GSM;
@@ -579,6 +573,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
   for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
     const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
     if (!A.is_lr(ic, k)) continue;
+    if (only_dense_operands && A.is_lr(ic, i) && A.is_lr(i, k)) continue;
     const int blk = ic * A.nb + k;
     const int bc = A.bs(ic), bk = A.bs(k);
     const int kc = A.rank[blk];
@@ -777,6 +772,338 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
 }
 
 // ---------------------------------------------------------------------------
+// K4' (mixed path): recompression by Gram matrices.  Same update and the same
+// core truncation (RRQR + RQ of the core, or its fixed rank) as k_recompress,
+// but the stacked bases A = [U_C | U_L] and B = [Vt_C | V_U] are not
+// factored along their b rows: their FP64 Gram matrices A^T A, B^T B (one
+// GEMM pass over the FP32 bases) are factored by pivoted Cholesky,
+// A Pa ~= Qa [Ra11 Ra12] with Qa = A Pa(:, :ra) Ra11^{-1}, dropping directions
+// whose relative norm is below sqrt(gram_tol); the core is
+// M = Ra Pa^T blockdiag(S_C, T) Pb Rb^T and the new bases are
+// U = A Pa [Ra11^{-1} Q_core; 0], V^T = B Pb [Rb11^{-1} V_core; 0].
+// A Gram matrix in FP64 resolves directions down to ~1e-8 of the basis norm,
+// which is ample for the loose factor tolerance of the mixed path (the FP64
+// path keeps the Householder kernel).  Targets with a dense operand are left
+// to k_recompress.  256 threads; small matrices in shared memory when they fit.
+// ---------------------------------------------------------------------------
+constexpr int GRAM_THREADS = 256;
+constexpr int GRAM_SMEM_BYTES = 110 * 1024;
+constexpr int GRAM_REGION = GRAM_SMEM_BYTES / 8;
+
+// Per-CTA global scratch of the Gram kernel (used for the small matrices when
+// they do not fit shared memory, and for the tall outputs).
+struct GramLayout {
+  int64_t ga, gb, m1, m2, m3, m4, vec, uo, vo, tm, total;
+};
+
+FRANK_HD GramLayout gram_layout(int bmax, int smax) {
+  GramLayout L;
+  int64_t o = 0;
+  auto take = [&](int64_t n) { int64_t r = o; o += (n + 31) & ~int64_t(31); return r; };
+  L.ga = take((int64_t)smax * smax);
+  L.gb = take((int64_t)smax * smax);
+  L.m1 = take((int64_t)smax * smax);
+  L.m2 = take((int64_t)smax * smax);
+  L.m3 = take((int64_t)smax * smax);
+  L.m4 = take((int64_t)smax * smax);
+  L.vec = take(16 * (int64_t)smax);
+  L.uo = take((int64_t)bmax * smax);
+  L.vo = take((int64_t)bmax * smax);
+  L.tm = take((int64_t)bmax * bmax);
+  L.total = o;
+  return L;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GRAM_THREADS) k_recompress_gram(BlrView<T> A, FactorWs<T> ws, int i, int smax,
+                                                                  double core_scale, double gram_tol) {
+  extern __shared__ double region[];
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ double red[32];
+  __shared__ int s_redi[32];
+  __shared__ int s_r[3];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int m = A.nb - i - 1;
+  const int ld = A.bmax;
+  const int bi = A.bs(i);
+  const GramLayout L = gram_layout(A.bmax, smax);
+  double* base = ws.rscratch + (int64_t)blockIdx.x * ws.rscratch_stride;
+  for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
+    const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
+    if (!A.is_lr(ic, k) || !A.is_lr(ic, i) || !A.is_lr(i, k)) continue;
+    const int blk = ic * A.nb + k;
+    const int bc = A.bs(ic), bk = A.bs(k);
+    const int kc = A.rank[blk];
+    const int p = A.rank[ic * A.nb + i], q = A.rank[i * A.nb + k];
+    const int su = kc + p, sv = kc + q;
+    if (su > smax || sv > smax) {
+      if (threadIdx.x == 0) atomicAdd(ws.err + ERR_BOUNDS, 1);
+      continue;
+    }
+    const T* Uc = A.u(ic, k);
+    const T* Sc = A.s(ic, k);
+    const T* Vc = A.vt(ic, k);
+    const T* UL = A.u(ic, i);
+    const T* VU = A.vt(i, k);
+    const T* WL = ws.WL + (int64_t)ic * ld * ld;
+    const T* WU = ws.WU + (int64_t)k * ld * ld;
+    const int sm_ = su > sv ? su : sv;
+    // small matrices: Ga (su^2), Gb (sv^2), M1, M2 (su*sv), M3, M4 (sv*sv), vec;
+    // all in shared memory when they fit (then also the V-side temporaries)
+    const int64_t sq = (int64_t)sm_ * sm_;
+    const int64_t need = 6 * sq + 16 * (int64_t)sm_;
+    const bool in_sm = need <= GRAM_REGION;
+    double *Ga, *Gb, *M1, *M2, *M3, *M4, *vec;
+    if (in_sm) {
+      Ga = region; Gb = Ga + sq; M1 = Gb + sq; M2 = M1 + sq; M3 = M2 + sq; M4 = M3 + sq; vec = M4 + sq;
+    } else {
+      Ga = base + L.ga; Gb = base + L.gb; M1 = base + L.m1; M2 = base + L.m2; M3 = base + L.m3; M4 = base + L.m4;
+      vec = base + L.vec;
+    }
+    int* pa = reinterpret_cast<int*>(vec);
+    int* pb = pa + sm_;
+    int* jp = pb + sm_;
+    int* ji = jp + sm_;
+    double* tc = vec + 2 * (int64_t)sm_;
+    double* cn = tc + sm_;
+    double* pn = cn + sm_;
+    double* tc2 = pn + sm_;
+    double* Tm = base + L.tm;
+    double* Uo = base + L.uo;
+    double* Vo = base + L.vo;
+    // small targets: warp-level factorizations in shared memory; large ones:
+    // CTA-level factorizations
+    const bool small = in_sm && su <= 64 && sv <= 64;
+    const int cls = small ? 0 : 1;
+    PHASE_BEGIN();
+#ifdef FRANK_PHASE_TIMING
+    if (threadIdx.x == 0) atomicAdd(&g_phase_count[cls], 1ull);
+#endif
+    // T = -WL^T WU (p x q); Gram matrices of the stacked bases (upper blocks)
+    // skinny products: warp dot products when small, tiled GEMM otherwise
+    auto tn = [&](int mm_, int nn_, int kk_, double al, const T* Ap, const T* Bp, double* Cp, int ldc_) {
+      if ((int64_t)mm_ * nn_ <= 1024) cta_gemm_tn_dot(mm_, nn_, kk_, al, Ap, ld, Bp, ld, Cp, ldc_);
+      else cta_gemm<double, GRAM_THREADS>(mm_, nn_, kk_, al, Ap, ld, true, Bp, ld, false, 0.0, Cp, ldc_, gsm);
+    };
+    tn(p, q, bi, -1.0, WL, WU, Tm, p);
+    tn(kc, kc, bc, 1.0, Uc, Uc, Ga, su);
+    tn(kc, p, bc, 1.0, Uc, UL, Ga + (int64_t)kc * su, su);
+    tn(p, p, bc, 1.0, UL, UL, Ga + kc + (int64_t)kc * su, su);
+    tn(kc, kc, bk, 1.0, Vc, Vc, Gb, sv);
+    tn(kc, q, bk, 1.0, Vc, VU, Gb + (int64_t)kc * sv, sv);
+    tn(q, q, bk, 1.0, VU, VU, Gb + kc + (int64_t)kc * sv, sv);
+    for (int e = threadIdx.x; e < kc * p; e += blockDim.x) {
+      const int r = e % kc, c = e / kc;
+      Ga[(kc + c) + (int64_t)r * su] = Ga[r + (int64_t)(kc + c) * su];
+    }
+    for (int e = threadIdx.x; e < kc * q; e += blockDim.x) {
+      const int r = e % kc, c = e / kc;
+      Gb[(kc + c) + (int64_t)r * sv] = Gb[r + (int64_t)(kc + c) * sv];
+    }
+    __syncthreads();
+    PHASE_MARK(cls, 0);
+    // pivoted Cholesky of both Gram matrices (one warp each when small)
+    if (small) {
+      if (wid == 0) {
+        const int r_ = warp_pivoted_cholesky(su, Ga, su, pa, gram_tol, su);
+        if (lane == 0) s_r[0] = r_;
+      } else if (wid == 1) {
+        const int r_ = warp_pivoted_cholesky(sv, Gb, sv, pb, gram_tol, sv);
+        if (lane == 0) s_r[1] = r_;
+      }
+    } else {
+      const int r0 = cta_pivoted_cholesky(su, Ga, su, pa, gram_tol, su, red, s_redi);
+      const int r1 = cta_pivoted_cholesky(sv, Gb, sv, pb, gram_tol, sv, red, s_redi);
+      if (threadIdx.x == 0) { s_r[0] = r0; s_r[1] = r1; }
+    }
+    __syncthreads();
+    PHASE_MARK(cls, 1);
+    const int ra = s_r[0], rb = s_r[1];
+    // M1 = Pa^T blockdiag(S_C, T) Pb (su x sv); zero the lower parts of Ra, Rb
+    for (int64_t e = threadIdx.x; e < (int64_t)su * sv; e += blockDim.x) {
+      const int r = e % su, c = e / su;
+      const int orr = pa[r], occ = pb[c];
+      double v = 0.0;
+      if (orr < kc && occ < kc) v = double(Sc[orr + (int64_t)occ * A.kcap]);
+      else if (orr >= kc && occ >= kc) v = Tm[(orr - kc) + (int64_t)(occ - kc) * p];
+      M1[e] = v;
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)ra * su; e += blockDim.x) {
+      const int r = e % ra, c = e / ra;
+      if (r > c) Ga[r + (int64_t)c * su] = 0.0;
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)rb * sv; e += blockDim.x) {
+      const int r = e % rb, c = e / rb;
+      if (r > c) Gb[r + (int64_t)c * sv] = 0.0;
+    }
+    __syncthreads();
+    // M2 (ra x sv) = Ra M1 ; Core = M1 <- M2 Rb^T (ra x rb)
+    for (int64_t e = threadIdx.x; e < (int64_t)ra * sv; e += blockDim.x) {
+      const int r = e % ra, c = e / ra;
+      double acc = 0.0;
+      for (int t = r; t < su; ++t) acc += Ga[r + (int64_t)t * su] * M1[t + (int64_t)c * su];
+      M2[e] = acc;
+    }
+    __syncthreads();
+    double* Core = M1;  // ra x rb, ld ra
+    for (int64_t e = threadIdx.x; e < (int64_t)ra * rb; e += blockDim.x) {
+      const int r = e % ra, c = e / ra;
+      double acc = 0.0;
+      for (int t = c; t < sv; ++t) acc += M2[r + (int64_t)t * ra] * Gb[c + (int64_t)t * sv];
+      Core[e] = acc;
+    }
+    double f = 0.0;
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (int64_t)ra * rb; e += blockDim.x) f += Core[e] * Core[e];
+    f = block_sum(f, red);
+    const double thr = ws.fixed_rank > 0 ? 0.0 : core_scale * ws.eps * sqrt(f);
+    const int maxr = ws.fixed_rank > 0 ? min(ws.fixed_rank, A.kcap) : A.kcap;
+    PHASE_MARK(cls, 2);
+    if (small) {
+      if (wid == 0) {
+        const int r_ = (ra > 0 && rb > 0) ? warp_truncated_geqp3(ra, rb, Core, ra, thr, maxr, tc, cn, pn, jp) : 0;
+        if (lane == 0) s_r[2] = r_;
+      }
+    } else {
+      const int r_ = (ra > 0 && rb > 0) ? cta_truncated_geqp3(ra, rb, Core, ra, thr, maxr, tc, cn, pn, jp, red, s_redi)
+                                        : 0;
+      if (threadIdx.x == 0) s_r[2] = r_;
+    }
+    __syncthreads();
+    PHASE_MARK(cls, 3);
+    const int r = s_r[2];
+    if (r == 0) {
+      T* Uw = A.u(ic, k); T* Vw = A.vt(ic, k); T* Sw = A.s(ic, k);
+      for (int e = threadIdx.x; e < bc; e += blockDim.x) Uw[e] = T(e == 0 ? 1.0 : 0.0);
+      for (int e = threadIdx.x; e < bk; e += blockDim.x) Vw[e] = T(e == 0 ? 1.0 : 0.0);
+      if (threadIdx.x == 0) { Sw[0] = T(0); A.rank[blk] = 1; atomicAdd(ws.err + ERR_RECOMP, 1); }
+      __syncthreads();
+      continue;
+    }
+    if (threadIdx.x == 0) {
+      if (ws.fixed_rank == 0 && r >= A.kcap && r < min(ra, rb)) atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1);
+      atomicMax(ws.err + ERR_MAX_RANK, r);
+      atomicAdd(ws.err + ERR_RECOMP, 1);
+      atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)rounded_addition_flops(bc, bk, bi, kc, p, q, r));
+    }
+    double* X1 = M2;   // ra x r (M2 no longer needed)
+    double* X2 = M3;   // rb x r
+    double* Qt = M4;   // rb x r
+    double* Yk = M4;   // Qt with its columns reversed in place
+    T* Sw = A.s(ic, k);
+    if (small) {
+      if (wid == 0) {
+        // X1 = Ra11^{-1} Q_core
+        for (int e = lane; e < ra * r; e += 32) X1[e] = ((e % ra) == (e / ra)) ? 1.0 : 0.0;
+        __syncwarp();
+        warp_apply_q(ra, r, Core, ra, tc, r, X1, ra);
+        warp_upper_solve(ra, Ga, su, r, X1, ra);
+      } else if (wid == 1) {
+        // RQ of the kept rows R_core Pcore^T (r x rb): QR of X2 = (R_perm)^T J
+        for (int c = lane; c < rb; c += 32) ji[jp[c]] = c;
+        __syncwarp();
+        for (int e = lane; e < rb * r; e += 32) {
+          const int c = e % rb, a = e / rb;
+          const int row = r - 1 - a, src = ji[c];
+          X2[e] = (row <= src) ? Core[row + (int64_t)src * ra] : 0.0;
+        }
+        __syncwarp();
+        warp_householder_qr(rb, r, X2, rb, tc2);
+        for (int e = lane; e < r * r; e += 32) {
+          const int a = e % r, c = e / r;
+          const int ra_ = r - 1 - c, ca = r - 1 - a;
+          Sw[a + (int64_t)c * A.kcap] = T((ra_ <= ca) ? X2[ra_ + (int64_t)ca * rb] : 0.0);
+        }
+        for (int e = lane; e < rb * r; e += 32) Qt[e] = ((e % rb) == (e / rb)) ? 1.0 : 0.0;
+        __syncwarp();
+        warp_apply_q(rb, r, X2, rb, tc2, r, Qt, rb);
+        for (int e = lane; e < rb * (r / 2); e += 32) {
+          const int rr = e % rb, a = e / rb;
+          const double t0 = Qt[rr + (int64_t)a * rb];
+          Qt[rr + (int64_t)a * rb] = Qt[rr + (int64_t)(r - 1 - a) * rb];
+          Qt[rr + (int64_t)(r - 1 - a) * rb] = t0;
+        }
+        __syncwarp();
+        warp_upper_solve(rb, Gb, sv, r, Yk, rb);
+      }
+      __syncthreads();
+    } else {
+      for (int64_t e = threadIdx.x; e < (int64_t)ra * r; e += blockDim.x) X1[e] = ((e % ra) == (e / ra)) ? 1.0 : 0.0;
+      for (int c = threadIdx.x; c < rb; c += blockDim.x) ji[jp[c]] = c;
+      __syncthreads();
+      cta_apply_q(ra, r, Core, ra, tc, r, X1, (int64_t)ra);
+      for (int64_t e = threadIdx.x; e < (int64_t)rb * r; e += blockDim.x) {
+        const int c = e % rb, a = e / rb;
+        const int row = r - 1 - a, src = ji[c];
+        X2[e] = (row <= src) ? Core[row + (int64_t)src * ra] : 0.0;
+      }
+      __syncthreads();
+      cta_householder_qr(rb, r, X2, rb, tc2, red);
+      for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
+        const int a = e % r, c = e / r;
+        const int ra_ = r - 1 - c, ca = r - 1 - a;
+        Sw[a + (int64_t)c * A.kcap] = T((ra_ <= ca) ? X2[ra_ + (int64_t)ca * rb] : 0.0);
+      }
+      for (int64_t e = threadIdx.x; e < (int64_t)rb * r; e += blockDim.x) Qt[e] = ((e % rb) == (e / rb)) ? 1.0 : 0.0;
+      __syncthreads();
+      cta_apply_q(rb, r, X2, rb, tc2, r, Qt, (int64_t)rb);
+      for (int64_t e = threadIdx.x; e < (int64_t)rb * (r / 2); e += blockDim.x) {
+        const int rr = e % rb, a = e / rb;
+        const double t0 = Qt[rr + (int64_t)a * rb];
+        Qt[rr + (int64_t)a * rb] = Qt[rr + (int64_t)(r - 1 - a) * rb];
+        Qt[rr + (int64_t)(r - 1 - a) * rb] = t0;
+      }
+      __syncthreads();
+      cta_upper_solve(ra, Ga, su, r, X1, ra);
+      cta_upper_solve(rb, Gb, sv, r, Yk, rb);
+    }
+    PHASE_MARK(cls, 4);
+    // scatter to the stacked order: Xf (su x r) reuses M1, Yf (sv x r) M3
+    double* Xf = M1;
+    double* Yf = M3;
+    for (int64_t e = threadIdx.x; e < (int64_t)su * r; e += blockDim.x) Xf[e] = 0.0;
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (int64_t)ra * r; e += blockDim.x) {
+      const int rr = e % ra, c = e / ra;
+      Xf[pa[rr] + (int64_t)c * su] = X1[e];
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)sv * r; e += blockDim.x) Yf[e] = 0.0;
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (int64_t)rb * r; e += blockDim.x) {
+      const int rr = e % rb, c = e / rb;
+      Yf[pb[rr] + (int64_t)c * sv] = Yk[e];
+    }
+    __syncthreads();
+    // new bases into temporaries (the target's own U, Vt are operands):
+    // U = Uc Xf[:kc] + UL Xf[kc:], V^T = Vc Yf[:kc] + VU Yf[kc:]
+    if (r <= 16) {
+      cta_gemm_tall(bc, r, kc, Uc, ld, Xf, su, Uo, bc, false);
+      cta_gemm_tall(bc, r, p, UL, ld, Xf + kc, su, Uo, bc, true);
+      cta_gemm_tall(bk, r, kc, Vc, ld, Yf, sv, Tm, bk, false);
+      cta_gemm_tall(bk, r, q, VU, ld, Yf + kc, sv, Tm, bk, true);
+    } else {
+      cta_gemm<double, GRAM_THREADS>(bc, r, kc, 1.0, Uc, ld, false, Xf, su, false, 0.0, Uo, bc, gsm);
+      cta_gemm<double, GRAM_THREADS>(bc, r, p, 1.0, UL, ld, false, Xf + kc, su, false, 1.0, Uo, bc, gsm);
+      cta_gemm<double, GRAM_THREADS>(bk, r, kc, 1.0, Vc, ld, false, Yf, sv, false, 0.0, Tm, bk, gsm);
+      cta_gemm<double, GRAM_THREADS>(bk, r, q, 1.0, VU, ld, false, Yf + kc, sv, false, 1.0, Tm, bk, gsm);
+    }
+    T* Uw = A.u(ic, k);
+    T* Vw = A.vt(ic, k);
+    for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+      const int rr = e % bc, c = e / bc;
+      Uw[rr + (int64_t)c * ld] = T(Uo[e]);
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+      const int rr = e % bk, c = e / bk;
+      Vw[rr + (int64_t)c * ld] = T(Tm[e]);
+    }
+    PHASE_MARK(cls, 5);
+    if (threadIdx.x == 0) A.rank[blk] = r;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Solve kernels.  z is the n x nrhs right-hand side / solution (T, ld n).
 // Forward (trsm(L, b, Lower), trsm.cpp:163-174 for a block column B):
 //   y_i = Linv_i P_i z_i ; z_j -= L(j,i) y_i for j > i.
@@ -801,19 +1128,34 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, Fact
   }
   __syncthreads();
   const bool tr = (which >= 2);
-  // row r of the result, per warp: lanes over the inner index
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int e = wid; e < b * nrhs; e += nw) {
-    const int r = e % b, c = e / b;
-    double s = 0.0;
-    for (int t = lane; t < b; t += 32) {
-      const double mv = tr ? double(Mx[t + (int64_t)r * ld]) : double(Mx[r + (int64_t)t * ld]);
-      s += mv * double(tmp[t + (int64_t)c * ld]);
+  if (!tr) {
+    // y = M tmp: threads over rows r (consecutive threads read consecutive
+    // rows of a column of M: coalesced), loop over the inner index.
+    // each element of M is read once for all right-hand sides (nrhs <= 8)
+    for (int r = threadIdx.x; r < b; r += blockDim.x) {
+      double acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+      for (int t = 0; t < b; ++t) {
+        const double mv = double(Mx[r + (int64_t)t * ld]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nrhs) acc[c] += mv * double(tmp[t + (int64_t)c * ld]);
+      }
+      for (int c = 0; c < nrhs; ++c) z[o + r + (int64_t)c * ldz] = T(acc[c]);
     }
-    s = warp_sum(s);
-    if (lane == 0) {
-      const int dst = (which == 3) ? perm[r] : r;
-      z[o + dst + (int64_t)c * ldz] = T(s);
+  } else {
+    // y = M^T tmp: a warp per output row r reads column r of M (contiguous).
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int e = wid; e < b * nrhs; e += nw) {
+      const int r = e % b, c = e / b;
+      double s = 0.0;
+      for (int t = lane; t < b; t += 32) s += double(Mx[t + (int64_t)r * ld]) * double(tmp[t + (int64_t)c * ld]);
+      s = warp_sum(s);
+      if (lane == 0) {
+        const int dst = (which == 3) ? perm[r] : r;
+        z[o + dst + (int64_t)c * ldz] = T(s);
+      }
     }
   }
 }
@@ -871,15 +1213,22 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_scatter(BlrView<T> A, i
     }
   } else {
     const T* Dm = A.dense(bi_, bj_);
-    for (int e = wid; e < bj * nrhs; e += nw) {
-      const int rr = e % bj, h = e / bj;
-      double s = 0.0;
-      for (int t = lane; t < bi; t += 32) {
-        const double dv = tr ? double(Dm[t + (int64_t)rr * ld]) : double(Dm[rr + (int64_t)t * ld]);
-        s += dv * double(z[oi + t + (int64_t)h * ldz]);
+    if (!tr) {
+      // z_j -= D z_i, threads over rows (coalesced columns of D)
+      for (int e = threadIdx.x; e < bj * nrhs; e += blockDim.x) {
+        const int rr = e % bj, h = e / bj;
+        double s = 0.0;
+        for (int t = 0; t < bi; ++t) s += double(Dm[rr + (int64_t)t * ld]) * double(z[oi + t + (int64_t)h * ldz]);
+        z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
       }
-      s = warp_sum(s);
-      if (lane == 0) z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+    } else {
+      for (int e = wid; e < bj * nrhs; e += nw) {
+        const int rr = e % bj, h = e / bj;
+        double s = 0.0;
+        for (int t = lane; t < bi; t += 32) s += double(Dm[t + (int64_t)rr * ld]) * double(z[oi + t + (int64_t)h * ldz]);
+        s = warp_sum(s);
+        if (lane == 0) z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+      }
     }
   }
 }

@@ -531,3 +531,333 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
 }
 
 }  // namespace frank
+
+namespace frank {
+
+// ---------------------------------------------------------------------------
+// Pivoted Cholesky (LAPACK dpstf2 order: pivot = largest remaining diagonal of
+// the Schur complement, stop when it drops to tol_rel * the largest initial
+// diagonal or after maxr steps) of the symmetric positive semi-definite n x n
+// matrix A (full storage, column-major, lda; FP64; shared or global memory),
+// in place with explicit symmetric row/column swaps.  On return rows 0..r-1
+// of A hold R (upper trapezoid, columns in pivoted order) with
+// A(piv, piv) ~= R^T R, piv[c] = original index of pivoted column c.
+// Returns r.
+// ---------------------------------------------------------------------------
+FRANK_D int cta_pivoted_cholesky(int n, double* A, int64_t lda, int* piv, double tol_rel, int maxr, double* red,
+                                 int* redi) {
+  for (int c = threadIdx.x; c < n; c += blockDim.x) piv[c] = c;
+  double dmax0;
+  {
+    double best = -1.0; int bi = -1;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const double d = A[t + (int64_t)t * lda];
+      if (d > best) { best = d; bi = t; }
+    }
+    block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &dmax0);
+  }
+  const double stop = tol_rel * dmax0;
+  const int rmax = min(n, maxr);
+  int j = 0;
+  for (; j < rmax; ++j) {
+    double best = -1.0; int bi = -1;
+    for (int t = j + threadIdx.x; t < n; t += blockDim.x) {
+      const double d = A[t + (int64_t)t * lda];
+      if (d > best) { best = d; bi = t; }
+    }
+    double dmax;
+    const int p = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &dmax);
+    if (!(dmax > stop) || dmax <= 0.0) break;
+    if (p != j) {
+      // swap columns j, p (all rows), then rows j, p (all columns)
+      for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        const double a = A[r + (int64_t)j * lda];
+        A[r + (int64_t)j * lda] = A[r + (int64_t)p * lda];
+        A[r + (int64_t)p * lda] = a;
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        const double a = A[j + (int64_t)c * lda];
+        A[j + (int64_t)c * lda] = A[p + (int64_t)c * lda];
+        A[p + (int64_t)c * lda] = a;
+      }
+      if (threadIdx.x == 0) { const int q = piv[j]; piv[j] = piv[p]; piv[p] = q; }
+      __syncthreads();
+    }
+    const double rjj = sqrt(A[j + (int64_t)j * lda]);
+    __syncthreads();
+    for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) A[j + (int64_t)c * lda] /= rjj;
+    if (threadIdx.x == 0) A[j + (int64_t)j * lda] = rjj;
+    __syncthreads();
+    // trailing Schur complement: A[t, c] -= R[j, t] R[j, c] for t, c > j
+    const int nt = n - j - 1;
+    for (int e = threadIdx.x; e < nt * nt; e += blockDim.x) {
+      const int t = j + 1 + e % nt, c = j + 1 + e / nt;
+      A[t + (int64_t)c * lda] -= A[j + (int64_t)t * lda] * A[j + (int64_t)c * lda];
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  return j;
+}
+
+// X (r x nc, ldx) := R11^{-1} X with R11 the leading r x r upper triangle of R
+// (ldr); one thread per column, back substitution.
+FRANK_D void cta_upper_solve(int r, const double* R, int64_t ldr, int nc, double* X, int64_t ldx) {
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    double* x = X + (int64_t)c * ldx;
+    for (int i = r - 1; i >= 0; --i) {
+      double s = x[i];
+      for (int t = i + 1; t < r; ++t) s -= R[i + (int64_t)t * ldr] * x[t];
+      x[i] = s / R[i + (int64_t)i * ldr];
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace frank
+
+namespace frank {
+
+// ---------------------------------------------------------------------------
+// Warp-level small dense factorizations (one warp, __syncwarp only).  Used on
+// matrices of a few dozen rows / columns held in shared memory, where a
+// block-wide barrier per column step would dominate.
+// ---------------------------------------------------------------------------
+FRANK_D void warp_argmax(double& v, int& idx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (ov > v || (ov == v && oi >= 0 && (idx < 0 || oi < idx))) { v = ov; idx = oi; }
+  }
+}
+
+// Pivoted Cholesky of the symmetric PSD n x n A (full storage, lda), in place
+// (same contract as cta_pivoted_cholesky).
+FRANK_D int warp_pivoted_cholesky(int n, double* A, int64_t lda, int* piv, double tol_rel, int maxr) {
+  const int lane = threadIdx.x & 31;
+  for (int c = lane; c < n; c += 32) piv[c] = c;
+  double d0 = -1.0; int i0 = -1;
+  for (int t = lane; t < n; t += 32) { const double d = A[t + (int64_t)t * lda]; if (d > d0) { d0 = d; i0 = t; } }
+  warp_argmax(d0, i0);
+  const double stop = tol_rel * d0;
+  const int rmax = min(n, maxr);
+  int j = 0;
+  for (; j < rmax; ++j) {
+    double dm = -1.0; int p = -1;
+    for (int t = j + lane; t < n; t += 32) { const double d = A[t + (int64_t)t * lda]; if (d > dm) { dm = d; p = t; } }
+    warp_argmax(dm, p);
+    if (!(dm > stop) || dm <= 0.0) break;
+    if (p != j) {
+      for (int r = lane; r < n; r += 32) {
+        const double a = A[r + (int64_t)j * lda]; A[r + (int64_t)j * lda] = A[r + (int64_t)p * lda]; A[r + (int64_t)p * lda] = a;
+      }
+      __syncwarp();
+      for (int c = lane; c < n; c += 32) {
+        const double a = A[j + (int64_t)c * lda]; A[j + (int64_t)c * lda] = A[p + (int64_t)c * lda]; A[p + (int64_t)c * lda] = a;
+      }
+      if (lane == 0) { const int q = piv[j]; piv[j] = piv[p]; piv[p] = q; }
+      __syncwarp();
+    }
+    const double rjj = sqrt(A[j + (int64_t)j * lda]);
+    __syncwarp();
+    for (int c = j + 1 + lane; c < n; c += 32) A[j + (int64_t)c * lda] /= rjj;
+    if (lane == 0) A[j + (int64_t)j * lda] = rjj;
+    __syncwarp();
+    // trailing Schur complement, lanes over columns c (each lane updates its column)
+    for (int c = j + 1 + lane; c < n; c += 32) {
+      const double rc = A[j + (int64_t)c * lda];
+      for (int t = j + 1; t < n; ++t) A[t + (int64_t)c * lda] -= A[j + (int64_t)t * lda] * rc;
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  return j;
+}
+
+// Householder reflector of x (length m, stride 1) in place (dlarfg); returns tau.
+FRANK_D double warp_larfg(int m, double* x) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int e = 1 + lane; e < m; e += 32) s += x[e] * x[e];
+  s = warp_sum(s);
+  const double alpha = x[0];
+  double t = 0.0;
+  if (s > 0.0) {
+    const double nrm = sqrt(alpha * alpha + s);
+    const double beta = alpha >= 0.0 ? -nrm : nrm;
+    t = (beta - alpha) / beta;
+    const double scal = 1.0 / (alpha - beta);
+    for (int e = 1 + lane; e < m; e += 32) x[e] *= scal;
+    __syncwarp();
+    if (lane == 0) x[0] = beta;
+  }
+  __syncwarp();
+  return t;
+}
+
+// apply H = I - t v v^T (v in column vcol, v_0 = 1 implicit, rows j..m-1) to
+// column c of A (rows j..m-1)
+FRANK_D void warp_apply_reflector(int j, int m, const double* v, double t, double* a) {
+  const int lane = threadIdx.x & 31;
+  double w = (lane == 0) ? a[j] : 0.0;
+  for (int e = j + 1 + lane; e < m; e += 32) w += v[e] * a[e];
+  w = warp_sum(w) * t;
+  if (lane == 0) a[j] -= w;
+  for (int e = j + 1 + lane; e < m; e += 32) a[e] -= w * v[e];
+  __syncwarp();
+}
+
+FRANK_D void warp_householder_qr(int m, int n, double* A, int64_t lda, double* tau) {
+  const int lane = threadIdx.x & 31;
+  const int kmin = min(m, n);
+  for (int j = 0; j < kmin; ++j) {
+    double* col = A + (int64_t)j * lda;
+    const double t = warp_larfg(m - j, col + j);
+    if (lane == 0) tau[j] = t;
+    if (t != 0.0)
+      for (int c = j + 1; c < n; ++c) warp_apply_reflector(j, m, col, t, A + (int64_t)c * lda);
+  }
+  __syncwarp();
+}
+
+// X (m x r) := Q X, Q = H_0 ... H_{k-1} from warp_householder_qr / geqp3.
+FRANK_D void warp_apply_q(int m, int k, const double* V, int64_t ldv, const double* tau, int r, double* X,
+                          int64_t ldx) {
+  for (int j = k - 1; j >= 0; --j) {
+    const double t = tau[j];
+    if (t == 0.0) continue;
+    for (int c = 0; c < r; ++c) warp_apply_reflector(j, m, V + (int64_t)j * ldv, t, X + (int64_t)c * ldx);
+  }
+}
+
+// Truncated column-pivoted QR (same contract as cta_truncated_geqp3).
+FRANK_D int warp_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr, int maxr, double* tau,
+                                 double* cnorm, double* partial, int* jpvt) {
+  const double dlamch_e = 1.1102230246251565e-16;
+  const double tol3z = sqrt(dlamch_e);
+  const int lane = threadIdx.x & 31;
+  const int mind = min(min(m, n), maxr);
+  for (int c = 0; c < n; ++c) {
+    double s = 0.0;
+    for (int r = lane; r < m; r += 32) s += A[r + (int64_t)c * lda] * A[r + (int64_t)c * lda];
+    s = warp_sum(s);
+    if (lane == 0) { cnorm[c] = sqrt(s); partial[c] = sqrt(s); jpvt[c] = c; }
+  }
+  __syncwarp();
+  double maxc = -1.0; int mi = -1;
+  for (int c = lane; c < n; c += 32) if (cnorm[c] > maxc) { maxc = cnorm[c]; mi = c; }
+  warp_argmax(maxc, mi);
+  int r = 0;
+  while (r < mind && maxc > thr) {
+    double best = -1.0; int kp = -1;
+    for (int c = r + lane; c < n; c += 32) if (cnorm[c] > best) { best = cnorm[c]; kp = c; }
+    warp_argmax(best, kp);
+    if (kp != r) {
+      for (int e = lane; e < m; e += 32) {
+        const double a = A[e + (int64_t)r * lda]; A[e + (int64_t)r * lda] = A[e + (int64_t)kp * lda]; A[e + (int64_t)kp * lda] = a;
+      }
+      if (lane == 0) {
+        double a = cnorm[r]; cnorm[r] = cnorm[kp]; cnorm[kp] = a;
+        a = partial[r]; partial[r] = partial[kp]; partial[kp] = a;
+        const int q = jpvt[r]; jpvt[r] = jpvt[kp]; jpvt[kp] = q;
+      }
+      __syncwarp();
+    }
+    double* col = A + (int64_t)r * lda;
+    double tt;
+    if (r < m - 1) tt = warp_larfg(m - r, col + r);
+    else tt = 0.0;
+    if (lane == 0) tau[r] = tt;
+    __syncwarp();
+    if (r < min(m, n) - 1 && tt != 0.0)
+      for (int c = r + 1; c < n; ++c) warp_apply_reflector(r, m, col, tt, A + (int64_t)c * lda);
+    // norm down-date (LAWN 176), lanes over columns
+    for (int c = r + 1 + lane; c < n; c += 32) {
+      if (cnorm[c] != 0.0) {
+        double temp = fabs(A[r + (int64_t)c * lda] / cnorm[c]);
+        temp = fmax(0.0, (1.0 - temp) * (1.0 + temp));
+        const double ratio = cnorm[c] / partial[c];
+        if (temp * ratio * ratio > tol3z) {
+          cnorm[c] = cnorm[c] * sqrt(temp);
+        } else {
+          double s2 = 0.0;
+          for (int e = r + 1; e < m; ++e) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
+          cnorm[c] = (r < m - 1) ? sqrt(s2) : 0.0;
+          partial[c] = cnorm[c];
+        }
+      }
+    }
+    __syncwarp();
+    ++r;
+    maxc = -1.0; mi = -1;
+    for (int c = r + lane; c < n; c += 32) if (cnorm[c] > maxc) { maxc = cnorm[c]; mi = c; }
+    warp_argmax(maxc, mi);
+    if (r >= n) maxc = 0.0;
+  }
+  __syncwarp();
+  return r;
+}
+
+// X (r x nc) := R11^{-1} X, R11 upper r x r; lanes over columns.
+FRANK_D void warp_upper_solve(int r, const double* R, int64_t ldr, int nc, double* X, int64_t ldx) {
+  const int lane = threadIdx.x & 31;
+  for (int c = lane; c < nc; c += 32) {
+    double* x = X + (int64_t)c * ldx;
+    for (int i = r - 1; i >= 0; --i) {
+      double s = x[i];
+      for (int t = i + 1; t < r; ++t) s -= R[i + (int64_t)t * ldr] * x[t];
+      x[i] = s / R[i + (int64_t)i * ldr];
+    }
+  }
+  __syncwarp();
+}
+
+// C (m x n, ldc, FP64) = alpha * A^T B with A (k x m), B (k x n) column-major
+// and k long (the rows of the bases): one warp per output, lanes over k.
+// Coalesced reads of columns of A and B; one block barrier at the end.
+template <typename TA, typename TB>
+FRANK_D void cta_gemm_tn_dot(int m, int n, int k, double alpha, const TA* A, int64_t lda, const TB* B, int64_t ldb,
+                             double* C, int64_t ldc) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int e = wid; e < m * n; e += nw) {
+    const int a = e % m, c = e / m;
+    const TA* pa = A + (int64_t)a * lda;
+    const TB* pb = B + (int64_t)c * ldb;
+    double s = 0.0;
+    for (int t = lane; t < k; t += 32) s += double(pa[t]) * double(pb[t]);
+    s = warp_sum(s);
+    if (lane == 0) C[a + (int64_t)c * ldc] = alpha * s;
+  }
+  __syncthreads();
+}
+
+// C (m x n, ldc) = A (m x k, lda) X (k x n, ldx, FP64) [+ C if accumulate],
+// m long (the rows of the bases), k and n small: threads over rows, each
+// thread keeps up to 8 outputs in registers per pass over X's columns.
+template <typename TA, typename TC>
+FRANK_D void cta_gemm_tall(int m, int n, int k, const TA* A, int64_t lda, const double* X, int64_t ldx, TC* C,
+                           int64_t ldc, bool accumulate) {
+  for (int c0 = 0; c0 < n; c0 += 8) {
+    const int nc = min(8, n - c0);
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+      double acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+      for (int t = 0; t < k; ++t) {
+        const double av = double(A[r + (int64_t)t * lda]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nc) acc[c] += av * X[t + (int64_t)(c0 + c) * ldx];
+      }
+      for (int c = 0; c < nc; ++c) {
+        TC* pc = C + r + (int64_t)(c0 + c) * ldc;
+        *pc = TC(accumulate ? double(*pc) + acc[c] : acc[c]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace frank

@@ -134,7 +134,11 @@ int frank_blr_get_pivots(const frank_blr* plan, int i, int* ipiv);
  *                            find_svd_truncation_rank -- the reference algorithm;
  *   "rounded_addition_rrqr"  (default) the reference's fixed-accuracy compressor
  *                            truncated_geqp3 + rq applied to the same core, with
- *                            tolerance core_scale * eps (core_scale <= 0: 0.1).
+ *                            tolerance core_scale * eps (core_scale <= 0: 0.1);
+ *   "rounded_addition_rrqr_gram"  mixed plans only: the same RRQR core, with the
+ *                            stacked bases orthogonalised through their FP64
+ *                            Gram matrices (pivoted Cholesky) instead of a
+ *                            Householder QR along the block rows.
  * Fixed-rank plans always use the core SVD. */
 int frank_blr_set_lra(frank_blr* plan, const char* name, double core_scale);
 

@@ -136,3 +136,26 @@ def test_mixed_precision_refinement_reaches_1e10(gpu_lib, dim):
     P.getrf()
     xp, itp, resp = P.refine(b, tol=1e-10, maxit=30)
     assert np.linalg.norm(xs - xp) / np.linalg.norm(xp) <= 1e-8
+
+
+@pytest.mark.parametrize("lra", ["rounded_addition_rrqr", "rounded_addition_rrqr_gram"])
+@pytest.mark.parametrize("feps", [1e-3, 1e-5])
+def test_mixed_factor_error_matches_oracle(gpu_lib, feps, lra):
+    """Mixed plan (FP32 bases, Gram-based recompression with the RRQR core):
+    factorization error within a factor 10 of the oracle's FP64 rounded
+    addition at the same tolerance, plus the FP32 floor (1e-6)."""
+    n, nb = 1024, 4
+    rng = np.random.default_rng(5)
+    x, _ = fo.morton_sort(rng.random((3, n)), 10)
+    A = fo.build_hierarchical(fo.laplacend, x, n, n // nb, nb, eps=1e-8)
+    A_dense = fo.to_dense(A)
+    fo.LRA_MODE["mode"] = "rounded_addition"
+    H = fo.build_hierarchical(fo.laplacend, x, n, n // nb, nb, eps=feps)
+    L, U = fo.getrf(fo.deep_copy(H))
+    Hd = fo.to_dense(H)
+    ref_ferr = np.linalg.norm(Hd - fo.to_dense(L) @ fo.to_dense(U)) / np.linalg.norm(Hd)
+    M = _upload(A, n, nb, eps=feps, precision="mixed")
+    M.set_lra(lra)
+    M.getrf()
+    gpu_ferr = _factor_error(A_dense, M)
+    assert gpu_ferr <= FACTOR * ref_ferr + 1e-6, (gpu_ferr, ref_ferr)
