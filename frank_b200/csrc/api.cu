@@ -270,29 +270,22 @@ template <typename T>
 int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cudaStream_t s) {
   BlrView<T> W = work_view<T>(p);
   FactorWs<T> ws = factor_ws<T>(p);
-  T* tmp = static_cast<T*>(p->stmp);
-  T* sct = static_cast<T*>(p->sctmp);
-  const size_t shm = (size_t)p->kcap * nrhs * sizeof(double);
+  T* ybuf = static_cast<T*>(p->stmp);
   const int nb = p->nb;
-  p->solve_launches += 4 * nb - 2;
+  const int gd = (p->bmax + SOLVE_ROWS - 1) / SOLVE_ROWS;
+  const size_t shd = ((size_t)p->bmax * nrhs + (size_t)(SOLVE_THREADS / SOLVE_ROWS) * SOLVE_ROWS * 8) * sizeof(double);
+  const size_t shs = ((size_t)p->bmax * nrhs + 2 * (size_t)p->kcap * nrhs) * sizeof(double);
+  p->solve_launches += 4 * nb;
+  auto step = [&](int i, int dmode, int smode, int ntarget) {
+    k_solve_diag<T><<<gd, SOLVE_THREADS, shd, s>>>(W, ws, i, z, ldz, nrhs, dmode, ybuf);
+    k_solve_scatter<T><<<ntarget + 1, SOLVE_THREADS, shs, s>>>(W, i, z, ldz, nrhs, smode, ybuf, ntarget);
+  };
   if (!transpose) {
-    for (int i = 0; i < nb; ++i) {
-      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 0, tmp);
-      if (nb - i - 1 > 0) k_solve_scatter<T><<<nb - i - 1, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 0, sct);
-    }
-    for (int i = nb - 1; i >= 0; --i) {
-      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 1, tmp);
-      if (i > 0) k_solve_scatter<T><<<i, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 1, sct);
-    }
+    for (int i = 0; i < nb; ++i) step(i, 0, 0, nb - i - 1);
+    for (int i = nb - 1; i >= 0; --i) step(i, 1, 1, i);
   } else {
-    for (int i = 0; i < nb; ++i) {
-      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 2, tmp);
-      if (nb - i - 1 > 0) k_solve_scatter<T><<<nb - i - 1, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 2, sct);
-    }
-    for (int i = nb - 1; i >= 0; --i) {
-      k_solve_diag<T><<<1, SOLVE_THREADS, 0, s>>>(W, ws, i, z, ldz, nrhs, 3, tmp);
-      if (i > 0) k_solve_scatter<T><<<i, SOLVE_THREADS, shm, s>>>(W, i, z, ldz, nrhs, 3, sct);
-    }
+    for (int i = 0; i < nb; ++i) step(i, 2, 2, nb - i - 1);
+    for (int i = nb - 1; i >= 0; --i) step(i, 3, 3, i);
   }
   CUDA_TRY(cudaGetLastError());
   return FRANK_OK;
@@ -567,9 +560,13 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   }
   // dynamic shared memory of the solve / matvec kernels (kcap * 8 RHS * 2 doubles)
   const int shm = (int)(2 * kc * 8 * sizeof(double));
+  const int shs = (int)((bm * 8 + 2 * kc * 8) * sizeof(double));
+  const int shd = (int)((bm * 8 + (SOLVE_THREADS / SOLVE_ROWS) * SOLVE_ROWS * 8) * sizeof(double));
   cudaFuncSetAttribute(k_matvec_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
-  cudaFuncSetAttribute(k_solve_scatter<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
-  cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  cudaFuncSetAttribute(k_solve_scatter<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
+  cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
+  cudaFuncSetAttribute(k_solve_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shd);
+  cudaFuncSetAttribute(k_solve_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shd);
   cudaFuncSetAttribute(k_recompress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, GRAM_SMEM_BYTES);

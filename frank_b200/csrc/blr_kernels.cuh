@@ -1111,123 +1111,192 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_recompress_gram(BlrView<T> A, 
 //   x_i = Uinv_i z_i ; z_j -= U(j,i) x_i for j < i.
 // ---------------------------------------------------------------------------
 constexpr int SOLVE_THREADS = 256;
+constexpr int SOLVE_ROWS = 64;   // rows of the diagonal solve per CTA
 
-// y = M * P(z_i) (or M z_i), in place in z_i; M = Linv or Uinv; tmp (bmax x nrhs)
+// y = M * P(z_i) (which 0: Linv, permuted input; 1: Uinv),
+// y = M^T z_i (2: Uinv^T), or y = P^T (Linv^T z_i) (3), into ybuf (ld bmax).
+// grid = ceil(b / SOLVE_ROWS) CTAs; each stages the whole input block in
+// shared memory (b x nrhs doubles) and produces SOLVE_ROWS rows.
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, FactorWs<T> ws, int i, T* z, int64_t ldz,
-                                                              int nrhs, int which, T* tmp) {
-  // which: 0 forward (Linv, permute first), 1 backward (Uinv),
-  //        2 transpose-forward (Uinv^T), 3 transpose-backward (P^T Linv^T)
+__global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, FactorWs<T> ws, int i, const T* z,
+                                                              int64_t ldz, int nrhs, int which, T* ybuf) {
+  extern __shared__ double xs[];          // b x nrhs input, then 4 x SOLVE_ROWS x nrhs partials
   const int b = A.bs(i), ld = A.bmax;
   const int64_t o = A.off[i];
   const T* Mx = (which == 0 || which == 3) ? ws.Linv + (int64_t)i * ld * ld : ws.Uinv + (int64_t)i * ld * ld;
   const int* perm = ws.perm + (int64_t)i * ld;
   for (int e = threadIdx.x; e < b * nrhs; e += blockDim.x) {
     const int r = e % b, c = e / b;
-    tmp[r + (int64_t)c * ld] = z[o + (which == 0 ? perm[r] : r) + (int64_t)c * ldz];
+    xs[e] = double(z[o + (which == 0 ? perm[r] : r) + (int64_t)c * ldz]);
   }
   __syncthreads();
-  const bool tr = (which >= 2);
-  if (!tr) {
-    // y = M tmp: threads over rows r (consecutive threads read consecutive
-    // rows of a column of M: coalesced), loop over the inner index.
-    // each element of M is read once for all right-hand sides (nrhs <= 8)
-    for (int r = threadIdx.x; r < b; r += blockDim.x) {
+  const int r0 = blockIdx.x * SOLVE_ROWS;
+  const int nr = min(SOLVE_ROWS, b - r0);
+  if (which <= 1) {
+    // rows r0.. of M x: thread (rl, sl) sums the inner slice sl of row rl
+    double* part = xs + (int64_t)b * nrhs;
+    const int rl = threadIdx.x % SOLVE_ROWS, sl = threadIdx.x / SOLVE_ROWS;  // 4 slices
+    const int nsl = SOLVE_THREADS / SOLVE_ROWS;
+    const int tlen = (b + nsl - 1) / nsl;
+    const int t0 = sl * tlen, t1 = min(b, t0 + tlen);
+    double acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+    if (rl < nr) {
+      const T* mrow = Mx + r0 + rl;
+#pragma unroll 4
+      for (int t = t0; t < t1; ++t) {
+        const double mv = double(mrow[(int64_t)t * ld]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nrhs) acc[c] += mv * xs[t + c * b];
+      }
+    }
+    for (int c = 0; c < nrhs; ++c) part[(sl * SOLVE_ROWS + rl) * 8 + c] = acc[c];
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
+      const int r = e % nr, c = e / nr;
+      double s = 0.0;
+      for (int q = 0; q < nsl; ++q) s += part[(q * SOLVE_ROWS + r) * 8 + c];
+      ybuf[r0 + r + (int64_t)c * ld] = T(s);
+    }
+  } else {
+    // rows r0.. of M^T x: a warp per output row reads column r of M
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int rl = wid; rl < nr; rl += nw) {
+      const int r = r0 + rl;
+      const T* mcol = Mx + (int64_t)r * ld;
       double acc[8];
 #pragma unroll
       for (int c = 0; c < 8; ++c) acc[c] = 0.0;
-      for (int t = 0; t < b; ++t) {
-        const double mv = double(Mx[r + (int64_t)t * ld]);
+#pragma unroll 4
+      for (int t = lane; t < b; t += 32) {
+        const double mv = double(mcol[t]);
 #pragma unroll
         for (int c = 0; c < 8; ++c)
-          if (c < nrhs) acc[c] += mv * double(tmp[t + (int64_t)c * ld]);
+          if (c < nrhs) acc[c] += mv * xs[t + c * b];
       }
-      for (int c = 0; c < nrhs; ++c) z[o + r + (int64_t)c * ldz] = T(acc[c]);
-    }
-  } else {
-    // y = M^T tmp: a warp per output row r reads column r of M (contiguous).
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int e = wid; e < b * nrhs; e += nw) {
-      const int r = e % b, c = e / b;
-      double s = 0.0;
-      for (int t = lane; t < b; t += 32) s += double(Mx[t + (int64_t)r * ld]) * double(tmp[t + (int64_t)c * ld]);
-      s = warp_sum(s);
-      if (lane == 0) {
-        const int dst = (which == 3) ? perm[r] : r;
-        z[o + dst + (int64_t)c * ldz] = T(s);
+      for (int c = 0; c < nrhs; ++c) {
+        const double sum = warp_sum(acc[c]);
+        if (lane == 0) ybuf[(which == 3 ? perm[r] : r) + (int64_t)c * ld] = T(sum);
       }
     }
   }
 }
 
-// z_j -= Blk(j,i) * z_i for j in the target set (one CTA per target block j).
+// z_j -= Blk z_i using the solved block y_i in ybuf, for every target j of
+// the step (one CTA each); CTA number `ntarget` copies y_i into z_i.
 // mode 0: targets j > i using blocks (j, i)        [forward, L]
 // mode 1: targets j < i using blocks (j, i)        [backward, U]
 // mode 2: targets j > i using blocks (i, j)^T      [transpose forward, U^T]
 // mode 3: targets j < i using blocks (i, j)^T      [transpose backward, L^T]
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_scatter(BlrView<T> A, int i, T* z, int64_t ldz, int nrhs,
-                                                                 int mode, T* tmpbase) {
-  const int j = (mode == 0 || mode == 2) ? i + 1 + blockIdx.x : (int)blockIdx.x;
+                                                                 int mode, const T* ybuf, int ntarget) {
+  extern __shared__ double ssm[];   // y_i (bi x nrhs), t1, t2 (kcap x nrhs each)
   const int ld = A.bmax;
-  const int bj = A.bs(j), bi = A.bs(i);
-  const int64_t oj = A.off[j], oi = A.off[i];
+  const int bi = A.bs(i);
+  const int64_t oi = A.off[i];
+  if ((int)blockIdx.x == ntarget) {
+    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+      const int r = e % bi, c = e / bi;
+      z[oi + r + (int64_t)c * ldz] = ybuf[r + (int64_t)c * ld];
+    }
+    return;
+  }
+  const int j = (mode == 0 || mode == 2) ? i + 1 + blockIdx.x : (int)blockIdx.x;
+  const int bj = A.bs(j);
+  const int64_t oj = A.off[j];
   const bool tr = (mode >= 2);
   const int bi_ = tr ? i : j, bj_ = tr ? j : i;  // block (bi_, bj_)
-  T* tmp = tmpbase + (int64_t)blockIdx.x * ld * 8;  // kcap x nrhs (nrhs <= 8)
-  extern __shared__ double ssm[];  // kcap * nrhs doubles
+  double* ys = ssm;
+  double* t1 = ys + (int64_t)bi * nrhs;
+  double* t2 = t1 + (int64_t)A.kcap * nrhs;
+  for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+    const int r = e % bi, c = e / bi;
+    ys[e] = double(ybuf[r + (int64_t)c * ld]);
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (A.is_lr(bi_, bj_)) {
     const int r = A.rank[bi_ * A.nb + bj_];
     const T* U = A.u(bi_, bj_);
     const T* S = A.s(bi_, bj_);
     const T* V = A.vt(bi_, bj_);
-    // non-transposed: z_j -= U S V^T z_i ; transposed: z_j -= V S^T U^T z_i
-    const T* inner = tr ? U : V;      // contracted with z_i (length bi)
+    const T* inner = tr ? U : V;      // contracted with y_i (length bi)
     const T* outer = tr ? V : U;      // expands to length bj
-    // t1 = inner^T z_i  (r x nrhs)
-    for (int e = wid; e < r * nrhs; e += nw) {
-      const int c = e % r, h = e / r;
-      double s = 0.0;
-      for (int t = lane; t < bi; t += 32) s += double(inner[t + (int64_t)c * ld]) * double(z[oi + t + (int64_t)h * ldz]);
-      s = warp_sum(s);
-      if (lane == 0) ssm[c + h * r] = s;
+    for (int cc = wid; cc < r; cc += nw) {
+      const T* col = inner + (int64_t)cc * ld;
+      double acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+#pragma unroll 4
+      for (int t = lane; t < bi; t += 32) {
+        const double v = double(col[t]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nrhs) acc[c] += v * ys[t + c * bi];
+      }
+      for (int c = 0; c < nrhs; ++c) {
+        const double sum = warp_sum(acc[c]);
+        if (lane == 0) t1[cc + c * r] = sum;
+      }
     }
     __syncthreads();
-    // t2 = S t1 (or S^T t1)
     for (int e = threadIdx.x; e < r * nrhs; e += blockDim.x) {
       const int c = e % r, h = e / r;
-      double s = 0.0;
+      double sacc = 0.0;
       for (int t = 0; t < r; ++t) {
         const double sv = tr ? double(S[t + (int64_t)c * A.kcap]) : double(S[c + (int64_t)t * A.kcap]);
-        s += sv * ssm[t + h * r];
+        sacc += sv * t1[t + h * r];
       }
-      tmp[c + (int64_t)h * ld] = T(s);
+      t2[c + h * r] = sacc;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < bj * nrhs; e += blockDim.x) {
-      const int rr = e % bj, h = e / bj;
-      double s = 0.0;
-      for (int t = 0; t < r; ++t) s += double(outer[rr + (int64_t)t * ld]) * double(tmp[t + (int64_t)h * ld]);
-      z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+    for (int rr = threadIdx.x; rr < bj; rr += blockDim.x) {
+      double acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+#pragma unroll 4
+      for (int t = 0; t < r; ++t) {
+        const double ov = double(outer[rr + (int64_t)t * ld]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nrhs) acc[c] += ov * t2[t + c * r];
+      }
+      for (int c = 0; c < nrhs; ++c) z[oj + rr + (int64_t)c * ldz] = T(double(z[oj + rr + (int64_t)c * ldz]) - acc[c]);
     }
   } else {
     const T* Dm = A.dense(bi_, bj_);
     if (!tr) {
-      // z_j -= D z_i, threads over rows (coalesced columns of D)
-      for (int e = threadIdx.x; e < bj * nrhs; e += blockDim.x) {
-        const int rr = e % bj, h = e / bj;
-        double s = 0.0;
-        for (int t = 0; t < bi; ++t) s += double(Dm[rr + (int64_t)t * ld]) * double(z[oi + t + (int64_t)h * ldz]);
-        z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+      for (int rr = threadIdx.x; rr < bj; rr += blockDim.x) {
+        double acc[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+#pragma unroll 4
+        for (int t = 0; t < bi; ++t) {
+          const double dv = double(Dm[rr + (int64_t)t * ld]);
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < nrhs) acc[c] += dv * ys[t + c * bi];
+        }
+        for (int c = 0; c < nrhs; ++c) z[oj + rr + (int64_t)c * ldz] = T(double(z[oj + rr + (int64_t)c * ldz]) - acc[c]);
       }
     } else {
-      for (int e = wid; e < bj * nrhs; e += nw) {
-        const int rr = e % bj, h = e / bj;
-        double s = 0.0;
-        for (int t = lane; t < bi; t += 32) s += double(Dm[t + (int64_t)rr * ld]) * double(z[oi + t + (int64_t)h * ldz]);
-        s = warp_sum(s);
-        if (lane == 0) z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - s);
+      for (int rr = wid; rr < bj; rr += nw) {
+        double acc[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+        for (int t = lane; t < bi; t += 32) {
+          const double dv = double(Dm[t + (int64_t)rr * ld]);
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < nrhs) acc[c] += dv * ys[t + c * bi];
+        }
+        for (int c = 0; c < nrhs; ++c) {
+          const double sum = warp_sum(acc[c]);
+          if (lane == 0) z[oj + rr + (int64_t)c * ldz] = T(double(z[oj + rr + (int64_t)c * ldz]) - sum);
+        }
       }
     }
   }
