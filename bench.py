@@ -260,9 +260,10 @@ def bench_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-# Algorithmic FLOPs of the full workload's recompressions, measured by the GPU
-# run (kernel counters) at eps = 1e-8; used to scale the CPU sample.
-FULL_WORKLOAD_FLOPS = 1.46e13
+# Algorithmic FLOPs of the full workload's recompressions at eps = 1e-8, as
+# counted by the FP64 factorization's in-kernel counter (the same per-update
+# formula as run_cpu_sample's); used to scale the CPU sample.
+FULL_WORKLOAD_FLOPS = 2.578e13
 
 
 def profile_case(name):
@@ -341,7 +342,8 @@ def main():
         }
         if not args.no_cpu_baseline:
             t, fl, desc = run_cpu_sample()
-            scale = FULL_WORKLOAD_FLOPS / fl
+            full = fp["kt"][-1]["recompress"]["flops"] or FULL_WORKLOAD_FLOPS
+            scale = full / fl
             line["cpu_baseline"] = {"value": t * scale, "unit": "s", "cores": os.cpu_count(), "kind": "port",
                                     "sample": desc + "; %.2f s measured, scaled x%.1f by algorithmic FLOPs"
                                     % (t, scale)}

@@ -70,6 +70,18 @@ SIGNATURES = {
     "frank_blr_solve_transpose_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int, _vp]),
     "frank_blr_stats": (C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p]),
     "frank_blr_kernel_times": (C.c_int, [_vp, _dp, _dp]),
+    "frank_blr_set_grid": (C.c_int, [_vp, C.c_int]),
+    "frank_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
+    "frank_batch_destroy": (C.c_int, [_vp]),
+    "frank_batch_getrf": (C.c_int, [_vp, _vp]),
+    "frank_batch_refine_device": (C.c_int, [_vp, C.POINTER(C.c_void_p), C.c_int64, C.POINTER(C.c_void_p), C.c_int64,
+                                            C.c_int, C.c_double, C.c_int, _ip, _dp]),
+    "frank_blr_matvec_transpose_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int,
+                                                    _vp]),
+    "frank_blr_refine_transpose_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int,
+                                                    C.c_double, C.c_int, _ip, _dp, _vp]),
+    "frank_kernel_dtheta_contract": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int64, _dp, C.c_void_p, C.c_int64,
+                                               C.c_void_p, C.c_int64, C.c_int, _dp, _vp]),
     "frank_getrf_dense_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                             _vp]),
 }

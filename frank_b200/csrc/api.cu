@@ -230,6 +230,26 @@ int collect_times(frank_blr* p) {
   return FRANK_OK;
 }
 
+// Status, counters and timings of a factorization that has completed.
+int finish_factor(frank_blr* p) {
+  CUDA_TRY(cudaMemcpy(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(p->flops_h, p->flops, FLOP_SLOTS * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  p->factored = true;
+  p->solve_launches = 0;
+  {
+    int rc = collect_times(p);
+    if (rc) return rc;
+  }
+  if (p->err_h[ERR_SINGULAR_STEP] != 0) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "zero pivot in the leaf getrf of diagonal block %d", p->err_h[ERR_SINGULAR_STEP] - 1);
+    return fail(FRANK_ERR_SINGULAR, buf);
+  }
+  if (p->err_h[ERR_BOUNDS] != 0) return fail(FRANK_ERR_INVALID, "stacked rank exceeded the recompression scratch");
+  if (p->err_h[ERR_RANK_OVERFLOW] != 0) return fail(FRANK_ERR_RANK_OVERFLOW, "a recompressed rank exceeded max_rank and was clamped");
+  return FRANK_OK;
+}
+
 template <typename T>
 int run_factor(frank_blr* p, cudaStream_t s) {
   if (!p->graph_exec) {
@@ -245,23 +265,8 @@ int run_factor(frank_blr* p, cudaStream_t s) {
     CUDA_TRY(cudaGraphInstantiate(&p->graph_exec, g, 0));
   }
   CUDA_TRY(cudaGraphLaunch(p->graph_exec, s));
-  CUDA_TRY(cudaMemcpyAsync(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(cudaMemcpyAsync(p->flops_h, p->flops, FLOP_SLOTS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
-  p->factored = true;
-  p->solve_launches = 0;
-  {
-    int rc = collect_times(p);
-    if (rc) return rc;
-  }
-  if (p->err_h[ERR_SINGULAR_STEP] != 0) {
-    char buf[128];
-    snprintf(buf, sizeof buf, "zero pivot in the leaf getrf of diagonal block %d", p->err_h[ERR_SINGULAR_STEP] - 1);
-    return fail(FRANK_ERR_SINGULAR, buf);
-  }
-  if (p->err_h[ERR_BOUNDS] != 0) return fail(FRANK_ERR_INVALID, "stacked rank exceeded the recompression scratch");
-  if (p->err_h[ERR_RANK_OVERFLOW] != 0) return fail(FRANK_ERR_RANK_OVERFLOW, "a recompressed rank exceeded max_rank and was clamped");
-  return FRANK_OK;
+  return finish_factor(p);
 }
 
 // ---- solve --------------------------------------------------------------
@@ -316,13 +321,13 @@ int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool tra
 }
 
 int matvec_device_impl(frank_blr* p, const double* x, int64_t ldx, double* y, int64_t ldy, int nrhs,
-                       const double* bres, int64_t ldb, cudaStream_t s) {
+                       const double* bres, int64_t ldb, cudaStream_t s, bool transpose = false) {
   BlrView<double> H = h_view(p);
   for (int c0 = 0; c0 < nrhs; c0 += 8) {
     const int nr = std::min(8, nrhs - c0);
     const size_t shm = 2 * (size_t)p->kcap * nr * sizeof(double);
     p->solve_launches += 2;
-    k_matvec_blocks<<<dim3(p->nb, p->nb), MV_THREADS, shm, s>>>(H, x + c0 * ldx, ldx, nr, p->part);
+    k_matvec_blocks<<<dim3(p->nb, p->nb), MV_THREADS, shm, s>>>(H, x + c0 * ldx, ldx, nr, p->part, transpose ? 1 : 0);
     k_matvec_reduce<<<p->nb, 256, 0, s>>>(H, p->part, nr, bres ? bres + c0 * ldb : nullptr, ldb, y + c0 * ldy, ldy);
   }
   CUDA_TRY(cudaGetLastError());
@@ -345,8 +350,24 @@ int colnorms(frank_blr* p, const double* v, int64_t ldv, int nrhs, std::vector<d
   return FRANK_OK;
 }
 
+// Column norms in two halves for batched use: enqueue (kernel + async copy
+// to the plan's pinned mirror), then read after the stream has synchronised.
+int colnorms_enqueue(frank_blr* p, const double* v, int64_t ldv, int nrhs, cudaStream_t s) {
+  ++p->solve_launches;
+  k_colnorm2<<<p->nrm_blocks, 256, 0, s>>>(v, p->n, ldv, nrhs, p->nrm);
+  CUDA_TRY(cudaMemcpyAsync(p->nrm_h, p->nrm, sizeof(double) * p->nrm_blocks * nrhs, cudaMemcpyDeviceToHost, s));
+  return FRANK_OK;
+}
+
+void colnorms_read(const frank_blr* p, int nrhs, std::vector<double>& out) {
+  out.assign(nrhs, 0.0);
+  for (int b = 0; b < p->nrm_blocks; ++b)
+    for (int h = 0; h < nrhs; ++h) out[h] += p->nrm_h[b * nrhs + h];
+  for (auto& v2 : out) v2 = std::sqrt(v2);
+}
+
 int refine_device_impl(frank_blr* p, const double* b, int64_t ldb, double* x, int64_t ldx, int nrhs, double tol,
-                       int maxit, int* iters, double* resid, cudaStream_t s) {
+                       int maxit, int* iters, double* resid, cudaStream_t s, bool transpose = false) {
   if (!p->factored) return fail(FRANK_ERR_STATE, "refine before getrf");
   if (nrhs > 8) return fail(FRANK_ERR_UNSUPPORTED, "refine takes at most 8 right-hand sides per call");
   int rc;
@@ -355,17 +376,17 @@ int refine_device_impl(frank_blr* p, const double* b, int64_t ldb, double* x, in
   // x0 = (LU)^{-1} b
   CUDA_TRY(cudaMemcpy2DAsync(x, ldx * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
                              cudaMemcpyDeviceToDevice, s));
-  if ((rc = solve_device_impl(p, x, ldx, nrhs, false, s))) return rc;
+  if ((rc = solve_device_impl(p, x, ldx, nrhs, transpose, s))) return rc;
   double* r = p->vtmp;  // n x nrhs residual / correction
   int it = 0;
   double res = 0.0;
   for (;;) {
-    if ((rc = matvec_device_impl(p, x, ldx, r, p->n, nrhs, b, ldb, s))) return rc;
+    if ((rc = matvec_device_impl(p, x, ldx, r, p->n, nrhs, b, ldb, s, transpose))) return rc;
     if ((rc = colnorms(p, r, p->n, nrhs, rn, s))) return rc;
     res = 0.0;
     for (int h = 0; h < nrhs; ++h) res = std::max(res, rn[h] / (bn[h] > 0.0 ? bn[h] : 1.0));
     if (res <= tol || it >= maxit) break;
-    if ((rc = solve_device_impl(p, r, p->n, nrhs, false, s))) return rc;
+    if ((rc = solve_device_impl(p, r, p->n, nrhs, transpose, s))) return rc;
     ++p->solve_launches;
     k_axpy_cast<double><<<grid_for(p->n * nrhs), 256, 0, s>>>(r, p->n, x, ldx, p->n, nrhs);
     ++it;
@@ -898,6 +919,230 @@ int frank_blr_stats(const frank_blr* p, int64_t* launches, int64_t* recompressio
 }
 
 }  // extern "C"
+
+extern "C" int frank_blr_matvec_transpose_device(frank_blr* p, const double* d_x, int64_t ldx, double* d_y,
+                                                 int64_t ldy, int nrhs, void* stream) {
+  if (!p || !d_x || !d_y || nrhs < 1 || ldx < p->n || ldy < p->n) return fail(FRANK_ERR_INVALID, "bad matvec arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = matvec_device_impl(p, d_x, ldx, d_y, ldy, nrhs, nullptr, 0, s, true);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return FRANK_OK;
+}
+
+extern "C" int frank_blr_refine_transpose_device(frank_blr* p, const double* d_b, int64_t ldb, double* d_x,
+                                                 int64_t ldx, int nrhs, double tol, int maxit, int* iters,
+                                                 double* resid, void* stream) {
+  if (!p || !d_b || !d_x || nrhs < 1 || ldb < p->n || ldx < p->n || maxit < 0)
+    return fail(FRANK_ERR_INVALID, "bad refine arguments");
+  return refine_device_impl(p, d_b, ldb, d_x, ldx, nrhs, tol, maxit, iters, resid, static_cast<cudaStream_t>(stream),
+                            true);
+}
+
+extern "C" int frank_kernel_dtheta_contract(int kernel, const double* d_points, int dim, int64_t n,
+                                            const double* kparams, const double* d_lambda, int64_t ldl,
+                                            const double* d_x, int64_t ldx, int nrhs, double* out, void* stream) {
+  if (kernel != FRANK_KERNEL_EXP) return fail(FRANK_ERR_UNSUPPORTED, "dA/dtheta is defined for the exp kernel only");
+  if (!d_points || !kparams || !d_lambda || !d_x || !out || dim < 1 || dim > 3 || n < 1 || nrhs < 1 || nrhs > 8 ||
+      ldl < n || ldx < n || !(kparams[0] > 0.0))
+    return fail(FRANK_ERR_INVALID, "bad dtheta contraction arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t tiles = (n + DT_TILE - 1) / DT_TILE;
+  if (tiles > 65535) return fail(FRANK_ERR_UNSUPPORTED, "too many points for the contraction grid");
+  double* part = nullptr;
+  CUDA_TRY(cudaMalloc(&part, sizeof(double) * tiles * tiles));
+  k_dtheta_contract<<<dim3((unsigned)tiles, (unsigned)tiles), 256, 0, s>>>(d_points, dim, n, kparams[0], d_lambda, ldl,
+                                                                          d_x, ldx, nrhs, part);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> h((size_t)tiles * tiles);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(part);
+  if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  double acc = 0.0;
+  for (double v : h) acc += v;
+  *out = acc;
+  return FRANK_OK;
+}
+
+// ===========================================================================
+// Batches of independent systems (the batched uneven-systems workload):
+// every plan's factorization is one branch of a single captured graph, so
+// systems of different sizes run concurrently and the whole batch is one
+// graph launch; the batched refinement synchronises the host once per
+// iteration for all systems.
+// ===========================================================================
+struct frank_batch {
+  std::vector<frank_blr*> plans;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> streams;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+void free_batch(frank_batch* B) {
+  if (!B) return;
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  for (auto e : B->join) if (e) cudaEventDestroy(e);
+  if (B->fork) cudaEventDestroy(B->fork);
+  for (auto st : B->streams) if (st) cudaStreamDestroy(st);
+  if (B->stream) cudaStreamDestroy(B->stream);
+  delete B;
+}
+}  // namespace
+
+extern "C" int frank_blr_set_grid(frank_blr* p, int ctas) {
+  if (!p || ctas < 1) return fail(FRANK_ERR_INVALID, "bad grid");
+  cudaDeviceSynchronize();
+  const int nb = p->nb;
+  p->grid_recomp = std::max(1, std::min({nb * nb, p->sm_count - 1, ctas}));
+  p->grid_gram = std::max(1, std::min({nb * nb, 2 * (p->sm_count - 1), 2 * ctas}));
+  p->grid_dense = std::max(1, std::min({nb * nb, 2 * p->sm_count, ctas}));
+  if (p->rscratch) { cudaFree(p->rscratch); p->rscratch = nullptr; }
+  if (p->dscratch) { cudaFree(p->dscratch); p->dscratch = nullptr; }
+  CUDA_TRY(dalloc(&p->dscratch, (size_t)p->grid_dense * p->dstride));
+  if (p->nlr > 0)
+    CUDA_TRY(dalloc(&p->rscratch, (size_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
+                                      p->rstride));
+  if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
+  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  p->factored = false;
+  return FRANK_OK;
+}
+
+extern "C" int frank_batch_create(frank_blr* const* plans, int count, frank_batch** out) {
+  if (!plans || count < 1 || !out) return fail(FRANK_ERR_INVALID, "bad batch arguments");
+  for (int k = 0; k < count; ++k) {
+    if (!plans[k]) return fail(FRANK_ERR_INVALID, "null plan in batch");
+    if (plans[k]->precision != plans[0]->precision) return fail(FRANK_ERR_UNSUPPORTED, "mixed precisions in one batch");
+  }
+  frank_batch* B = new frank_batch();
+  B->plans.assign(plans, plans + count);
+  B->streams.assign(count, nullptr);
+  B->join.assign(count, nullptr);
+  bool ok = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int k = 0; ok && k < count; ++k)
+    ok = cudaStreamCreateWithFlags(&B->streams[k], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&B->join[k], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) { free_batch(B); return fail(FRANK_ERR_CUDA, "batch streams"); }
+  *out = B;
+  return FRANK_OK;
+}
+
+extern "C" int frank_batch_destroy(frank_batch* B) {
+  cudaDeviceSynchronize();
+  free_batch(B);
+  return FRANK_OK;
+}
+
+namespace {
+template <typename T>
+int batch_capture(frank_batch* B) {
+  cudaStream_t s = B->stream;
+  CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int rc = FRANK_OK;
+  cudaError_t e = cudaEventRecord(B->fork, s);
+  for (size_t k = 0; rc == FRANK_OK && e == cudaSuccess && k < B->plans.size(); ++k) {
+    e = cudaStreamWaitEvent(B->streams[k], B->fork, 0);
+    if (e == cudaSuccess) rc = enqueue_factor<T>(B->plans[k], B->streams[k]);
+    if (rc == FRANK_OK && e == cudaSuccess) e = cudaEventRecord(B->join[k], B->streams[k]);
+    if (rc == FRANK_OK && e == cudaSuccess) e = cudaStreamWaitEvent(s, B->join[k], 0);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  if (rc != FRANK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(FRANK_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  B->graph = g;
+  CUDA_TRY(cudaGraphInstantiate(&B->exec, g, 0));
+  return FRANK_OK;
+}
+}  // namespace
+
+extern "C" int frank_batch_getrf(frank_batch* B, void* stream) {
+  if (!B) return fail(FRANK_ERR_INVALID, "null batch");
+  (void)stream;
+  if (!B->exec) {
+    int rc = B->plans[0]->precision == FRANK_PREC_FP64 ? batch_capture<double>(B) : batch_capture<float>(B);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaGraphLaunch(B->exec, B->stream));
+  CUDA_TRY(cudaStreamSynchronize(B->stream));
+  int first = FRANK_OK;
+  for (frank_blr* p : B->plans) {
+    int rc = finish_factor(p);
+    if (rc && first == FRANK_OK) first = rc;
+  }
+  return first;
+}
+
+extern "C" int frank_batch_refine_device(frank_batch* B, const double* const* d_b, int64_t ldb, double* const* d_x,
+                                         int64_t ldx, int nrhs, double tol, int maxit, int* iters, double* resid) {
+  if (!B || !d_b || !d_x || nrhs < 1 || nrhs > 8 || maxit < 0) return fail(FRANK_ERR_INVALID, "bad batch refine arguments");
+  const int K = (int)B->plans.size();
+  for (int k = 0; k < K; ++k) {
+    frank_blr* p = B->plans[k];
+    if (!p->factored) return fail(FRANK_ERR_STATE, "batch refine before getrf");
+    if (ldb < p->n || ldx < p->n) return fail(FRANK_ERR_INVALID, "leading dimension below a system's order");
+  }
+  std::vector<std::vector<double>> bn(K);
+  std::vector<int> it(K, 0), done(K, 0);
+  std::vector<double> res(K, 0.0);
+  int rc;
+  for (int k = 0; k < K; ++k) if ((rc = colnorms_enqueue(B->plans[k], d_b[k], ldb, nrhs, B->streams[k]))) return rc;
+  for (int k = 0; k < K; ++k) {
+    CUDA_TRY(cudaStreamSynchronize(B->streams[k]));
+    colnorms_read(B->plans[k], nrhs, bn[k]);
+  }
+  for (int k = 0; k < K; ++k) {
+    frank_blr* p = B->plans[k];
+    CUDA_TRY(cudaMemcpy2DAsync(d_x[k], ldx * sizeof(double), d_b[k], ldb * sizeof(double), p->n * sizeof(double), nrhs,
+                               cudaMemcpyDeviceToDevice, B->streams[k]));
+    if ((rc = solve_device_impl(p, d_x[k], ldx, nrhs, false, B->streams[k]))) return rc;
+  }
+  for (;;) {
+    int active = 0;
+    for (int k = 0; k < K; ++k) {
+      if (done[k]) continue;
+      frank_blr* p = B->plans[k];
+      if ((rc = matvec_device_impl(p, d_x[k], ldx, p->vtmp, p->n, nrhs, d_b[k], ldb, B->streams[k]))) return rc;
+      if ((rc = colnorms_enqueue(p, p->vtmp, p->n, nrhs, B->streams[k]))) return rc;
+      ++active;
+    }
+    if (!active) break;
+    for (int k = 0; k < K; ++k) {
+      if (done[k]) continue;
+      frank_blr* p = B->plans[k];
+      CUDA_TRY(cudaStreamSynchronize(B->streams[k]));
+      std::vector<double> rn;
+      colnorms_read(p, nrhs, rn);
+      double r = 0.0;
+      for (int h = 0; h < nrhs; ++h) r = std::max(r, rn[h] / (bn[k][h] > 0.0 ? bn[k][h] : 1.0));
+      res[k] = r;
+      if (r <= tol || it[k] >= maxit) { done[k] = 1; continue; }
+      if ((rc = solve_device_impl(p, p->vtmp, p->n, nrhs, false, B->streams[k]))) return rc;
+      ++p->solve_launches;
+      k_axpy_cast<double><<<grid_for(p->n * nrhs), 256, 0, B->streams[k]>>>(p->vtmp, p->n, d_x[k], ldx, p->n, nrhs);
+      ++it[k];
+    }
+  }
+  for (int k = 0; k < K; ++k) CUDA_TRY(cudaStreamSynchronize(B->streams[k]));
+  int status = FRANK_OK;
+  for (int k = 0; k < K; ++k) {
+    if (iters) iters[k] = it[k];
+    if (resid) resid[k] = res[k];
+    if (res[k] > tol) status = FRANK_ERR_NOT_CONVERGED;
+  }
+  if (status) return fail(status, "a system of the batch reached maxit before the tolerance");
+  return FRANK_OK;
+}
 
 #ifdef FRANK_PHASE_TIMING
 // Read and clear the recompression phase counters (timing builds only).

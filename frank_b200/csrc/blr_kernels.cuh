@@ -1309,24 +1309,28 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_scatter(BlrView<T> A, i
 constexpr int MV_THREADS = 256;
 
 __global__ void __launch_bounds__(MV_THREADS) k_matvec_blocks(BlrView<double> H, const double* x, int64_t ldx,
-                                                              int nrhs, double* part) {
+                                                              int nrhs, double* part, int transpose) {
+  // part(i, j) = A(i, j) x_j, or A(j, i)^T x_j when transposing
   const int i = blockIdx.y, j = blockIdx.x;
   const int nb = H.nb, ld = H.bmax;
   const int bi = H.bs(i), bj = H.bs(j);
   const int64_t oj = H.off[j];
+  const int gi = transpose ? j : i, gj = transpose ? i : j;   // stored block (gi, gj)
   double* out = part + (int64_t)(i * nb + j) * ld * nrhs;
   extern __shared__ double t1[];   // 2 * kcap * nrhs doubles
   double* t2 = t1 + (int64_t)H.kcap * nrhs;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (H.is_lr(i, j)) {
-    const int r = H.rank[i * nb + j];
-    const double* U = H.u(i, j);
-    const double* S = H.s(i, j);
-    const double* V = H.vt(i, j);
+  if (H.is_lr(gi, gj)) {
+    const int r = H.rank[gi * nb + gj];
+    const double* U = H.u(gi, gj);
+    const double* S = H.s(gi, gj);
+    const double* V = H.vt(gi, gj);
+    const double* inner = transpose ? U : V;   // length bj (rows of x_j)
+    const double* outer = transpose ? V : U;   // length bi
     for (int e = wid; e < r * nrhs; e += nw) {
       const int c = e % r, h = e / r;
       double s = 0.0;
-      for (int t = lane; t < bj; t += 32) s += V[t + (int64_t)c * ld] * x[oj + t + (int64_t)h * ldx];
+      for (int t = lane; t < bj; t += 32) s += inner[t + (int64_t)c * ld] * x[oj + t + (int64_t)h * ldx];
       s = warp_sum(s);
       if (lane == 0) t1[c + h * r] = s;
     }
@@ -1334,23 +1338,36 @@ __global__ void __launch_bounds__(MV_THREADS) k_matvec_blocks(BlrView<double> H,
     for (int e = threadIdx.x; e < r * nrhs; e += blockDim.x) {
       const int c = e % r, h = e / r;
       double s = 0.0;
-      for (int t = 0; t < r; ++t) s += S[c + (int64_t)t * H.kcap] * t1[t + h * r];
+      for (int t = 0; t < r; ++t) {
+        const double sv = transpose ? S[t + (int64_t)c * H.kcap] : S[c + (int64_t)t * H.kcap];
+        s += sv * t1[t + h * r];
+      }
       t2[c + h * r] = s;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
       const int rr = e % bi, h = e / bi;
       double s = 0.0;
-      for (int t = 0; t < r; ++t) s += U[rr + (int64_t)t * ld] * t2[t + h * r];
+      for (int t = 0; t < r; ++t) s += outer[rr + (int64_t)t * ld] * t2[t + h * r];
       out[rr + (int64_t)h * ld] = s;
     }
   } else {
-    const double* Dm = H.dense(i, j);
-    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
-      const int rr = e % bi, h = e / bi;
-      double s = 0.0;
-      for (int t = 0; t < bj; ++t) s += Dm[rr + (int64_t)t * ld] * x[oj + t + (int64_t)h * ldx];
-      out[rr + (int64_t)h * ld] = s;
+    const double* Dm = H.dense(gi, gj);
+    if (!transpose) {
+      for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+        const int rr = e % bi, h = e / bi;
+        double s = 0.0;
+        for (int t = 0; t < bj; ++t) s += Dm[rr + (int64_t)t * ld] * x[oj + t + (int64_t)h * ldx];
+        out[rr + (int64_t)h * ld] = s;
+      }
+    } else {
+      for (int e = wid; e < bi * nrhs; e += nw) {
+        const int rr = e % bi, h = e / bi;
+        double s = 0.0;
+        for (int t = lane; t < bj; t += 32) s += Dm[t + (int64_t)rr * ld] * x[oj + t + (int64_t)h * ldx];
+        s = warp_sum(s);
+        if (lane == 0) out[rr + (int64_t)h * ld] = s;
+      }
     }
   }
 }
@@ -1400,6 +1417,51 @@ __global__ void k_axpy_cast(const TS* d, int64_t ldd, double* x, int64_t ldx, in
     const int64_t r = e % n, h = e / n;
     x[r + h * ldx] += double(d[r + h * ldd]);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint contraction for the exponential kernel A_ij = exp(-r_ij/theta) +
+// nugget*delta_ij: partial sums of sum_h sum_ij lambda_ih (dA_ij/dtheta) x_jh
+// with dA/dtheta = exp(-r/theta) r / theta^2, evaluated on the fly (the
+// kernel matrix is never formed).  64 x 64 tiles of point pairs per CTA,
+// points and vectors staged in shared memory; one partial per CTA, summed on
+// the host in a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int DT_TILE = 64;
+
+__global__ void __launch_bounds__(256) k_dtheta_contract(const double* x, int dim, int64_t n, double theta,
+                                                          const double* lam, int64_t ldl, const double* xv,
+                                                          int64_t ldx, int nrhs, double* partial) {
+  __shared__ double pi[3][DT_TILE], pj[3][DT_TILE];
+  __shared__ double li[8][DT_TILE], xj[8][DT_TILE];
+  __shared__ double red[32];
+  const int64_t i0 = (int64_t)blockIdx.y * DT_TILE, j0 = (int64_t)blockIdx.x * DT_TILE;
+  for (int e = threadIdx.x; e < DT_TILE * dim; e += blockDim.x) {
+    const int t = e % DT_TILE, d = e / DT_TILE;
+    pi[d][t] = (i0 + t < n) ? x[d * n + i0 + t] : 0.0;
+    pj[d][t] = (j0 + t < n) ? x[d * n + j0 + t] : 0.0;
+  }
+  for (int e = threadIdx.x; e < DT_TILE * nrhs; e += blockDim.x) {
+    const int t = e % DT_TILE, h = e / DT_TILE;
+    li[h][t] = (i0 + t < n) ? lam[i0 + t + h * ldl] : 0.0;
+    xj[h][t] = (j0 + t < n) ? xv[j0 + t + h * ldx] : 0.0;
+  }
+  __syncthreads();
+  double acc = 0.0;
+  const double inv_t2 = 1.0 / (theta * theta);
+  for (int e = threadIdx.x; e < DT_TILE * DT_TILE; e += blockDim.x) {
+    const int a = e % DT_TILE, c = e / DT_TILE;
+    if (i0 + a >= n || j0 + c >= n) continue;
+    double r2 = 0.0;
+    for (int d = 0; d < dim; ++d) { const double t = pi[d][a] - pj[d][c]; r2 += t * t; }
+    const double r = sqrt(r2);
+    const double da = exp(-r / theta) * r * inv_t2;
+    double w = 0.0;
+    for (int h = 0; h < nrhs; ++h) w += li[h][a] * xj[h][c];
+    acc += da * w;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = acc;
 }
 
 // ---------------------------------------------------------------------------

@@ -178,6 +178,41 @@ int frank_blr_refine_device(frank_blr* plan, const double* d_b, int64_t ldb, dou
  * the adjoint of solve(A, b) (no reference counterpart; python/FRANK adjoint). */
 int frank_blr_solve_transpose_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
 
+/* y = A_H^T x in FP64, and refinement of A_H^T x = b with the transposed
+ * solve (the adjoint solve A^T lambda = g of solve(A, b)).  No reference
+ * counterpart (python/FRANK adjoint). */
+int frank_blr_matvec_transpose_device(frank_blr* plan, const double* d_x, int64_t ldx, double* d_y, int64_t ldy,
+                                      int nrhs, void* stream);
+int frank_blr_refine_transpose_device(frank_blr* plan, const double* d_b, int64_t ldb, double* d_x, int64_t ldx,
+                                      int nrhs, double tol, int maxit, int* iters, double* resid, void* stream);
+
+/* out = sum_h sum_ij lambda_ih (dA_ij / dtheta) x_jh for the exponential
+ * kernel A_ij = exp(-r_ij / theta) + nugget delta_ij (kparams = {theta,
+ * nugget}), evaluated on the fly from the device points (dim x n,
+ * axis-major); the theta-gradient of a loss through solve(A(theta), b) is
+ * -out with lambda the adjoint solution.  No reference counterpart. */
+int frank_kernel_dtheta_contract(int kernel, const double* d_points, int dim, int64_t n, const double* kparams,
+                                 const double* d_lambda, int64_t ldl, const double* d_x, int64_t ldx, int nrhs,
+                                 double* out, void* stream);
+
+/* Limit a plan's recompression / update grids to `ctas` thread blocks and
+ * shrink its scratch accordingly, for plans that run concurrently in a batch. */
+int frank_blr_set_grid(frank_blr* plan, int ctas);
+
+/* A batch of independent plans (same precision): frank_batch_getrf factors
+ * all of them in one captured CUDA graph (one branch per system, so systems
+ * of uneven order run concurrently); frank_batch_refine_device refines every
+ * system k (b d_b[k], solution d_x[k], column-major, nrhs <= 8) to tol, the
+ * host synchronising once per iteration for the whole batch.  iters/resid
+ * are per system.  Replaces a host loop of getrf/trsm over independent
+ * Hierarchical matrices (no batched call in the reference). */
+typedef struct frank_batch frank_batch;
+int frank_batch_create(frank_blr* const* plans, int count, frank_batch** out);
+int frank_batch_destroy(frank_batch* batch);
+int frank_batch_getrf(frank_batch* batch, void* stream);
+int frank_batch_refine_device(frank_batch* batch, const double* const* d_b, int64_t ldb, double* const* d_x,
+                              int64_t ldx, int nrhs, double tol, int maxit, int* iters, double* resid);
+
 /* Counters of the last getrf: kernels launched by it plus those of every
  * solve / matvec / refine since, recompressions performed, the largest
  * recompressed rank and the number of ranks clamped at max_rank. */
