@@ -71,6 +71,7 @@ SIGNATURES = {
     "frank_blr_stats": (C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p]),
     "frank_blr_kernel_times": (C.c_int, [_vp, _dp, _dp]),
     "frank_blr_set_grid": (C.c_int, [_vp, C.c_int]),
+    "frank_blr_set_timing": (C.c_int, [_vp, C.c_int]),
     "frank_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
     "frank_batch_destroy": (C.c_int, [_vp]),
     "frank_batch_getrf": (C.c_int, [_vp, _vp]),

@@ -200,6 +200,11 @@ class BLRMatrix:
               "frank_blr_refine_device")
         return it.value, res.value
 
+    def set_timing(self, on: bool = True):
+        """Record per-class kernel times inside the factorization graph (off
+        by default: the event nodes serialise the graph's concurrent branches)."""
+        check(lib().frank_blr_set_timing(self._h, 1 if on else 0), "frank_blr_set_timing")
+
     def kernel_times(self) -> dict:
         """Per-class device time (ms) and algorithmic FLOPs of the last getrf."""
         ms = np.zeros(4)

@@ -88,6 +88,9 @@ struct frank_blr {
   // timing events recorded inside the captured graph: [step][class][begin,end]
   std::vector<cudaEvent_t> ev;
   double class_ms[FLOP_SLOTS] = {0};
+  bool timed = false;  // timing events recorded in the captured graph (opt-in:
+                       // event-record nodes serialise the graph's branches)
+  bool want_timing = false;
   // lookahead: second capture stream and its dependency events
   cudaStream_t aux = nullptr;
   cudaEvent_t fork = nullptr;
@@ -144,13 +147,23 @@ bool use_gram(const frank_blr* p) {
 
 cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * FLOP_SLOTS + cls) * 2 + end]; }
 
+// Per-CTA scratch of the update / recompression kernels, sized by the grids.
+int ensure_scratch(frank_blr* p) {
+  if (!p->dscratch) CUDA_TRY(dalloc(&p->dscratch, (size_t)p->grid_dense * p->dstride));
+  if (p->nlr > 0 && !p->rscratch)
+    CUDA_TRY(dalloc(&p->rscratch, (size_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
+                                      p->rstride));
+  return FRANK_OK;
+}
+
 // One factorization on stream s.  The leaf getrf of step i+1 runs on a second
 // stream (p->aux) as soon as step i's dense-target update has refreshed the
 // diagonal block (i+1, i+1), so it overlaps step i's recompressions
 // (lookahead of depth one); the panel of step i+1 waits for both.  The
 // recompression grid leaves one SM free for it.
 template <typename T>
-int enqueue_factor(frank_blr* p, cudaStream_t s) {
+int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
+  p->timed = timing;
   BlrView<double> H = h_view(p);
   BlrView<T> W = work_view<T>(p);
   FactorWs<T> ws = factor_ws<T>(p);
@@ -163,9 +176,9 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
   CUDA_TRY(cudaEventRecord(p->fork, s));
   CUDA_TRY(cudaStreamWaitEvent(s2, p->fork, 0));
   auto getrf_on_aux = [&](int step) -> int {
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 0), s2, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 0), s2, cudaEventRecordExternal));
     k_getrf<T><<<1, GETRF_THREADS, 0, s2>>>(W, ws, step);
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 1), s2, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 1), s2, cudaEventRecordExternal));
     CUDA_TRY(cudaEventRecord(p->getrf_done[step], s2));
     return FRANK_OK;
   };
@@ -176,20 +189,20 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
     CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[i], 0));
     const int m = p->nb - i - 1;
     if (m == 0) break;
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
     k_panel<T><<<2 * m, PANEL_THREADS, 0, s>>>(W, ws, i);
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 1), s, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 1), s, cudaEventRecordExternal));
     ++launches;
     const int mm = m * m;
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s, cudaEventRecordExternal));
     k_update_dense<T><<<std::min(mm, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
     ++launches;
     CUDA_TRY(cudaEventRecord(p->dense_done[i], s));
     CUDA_TRY(cudaStreamWaitEvent(s2, p->dense_done[i], 0));
     if ((rc = getrf_on_aux(i + 1))) return rc;
     ++launches;
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 0), s, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 0), s, cudaEventRecordExternal));
     if (p->nlr > 0) {
       if (use_gram(p)) {
         // mixed path: Gram-based recompression of every low-rank x low-rank
@@ -208,7 +221,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
         ++launches;
       }
     }
-    CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 1), s, cudaEventRecordExternal));
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 1), s, cudaEventRecordExternal));
   }
   CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[p->nb - 1], 0));
   CUDA_TRY(cudaGetLastError());
@@ -219,6 +232,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s) {
 // Per-class device time of the last factorization from the graph's events.
 int collect_times(frank_blr* p) {
   for (int c = 0; c < FLOP_SLOTS; ++c) p->class_ms[c] = 0.0;
+  if (!p->timed) return FRANK_OK;
   for (int i = 0; i < p->nb; ++i)
     for (int c = 0; c < FLOP_SLOTS; ++c) {
       if (i == p->nb - 1 && c != FLOP_GETRF) continue;
@@ -255,8 +269,10 @@ int run_factor(frank_blr* p, cudaStream_t s) {
   if (!p->graph_exec) {
     // Capture the whole step sequence once; kernel arguments are fixed
     // device pointers, ranks are read from device tables at run time.
+    int rc0 = ensure_scratch(p);
+    if (rc0) return rc0;
     CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_factor<T>(p, s);
+    int rc = enqueue_factor<T>(p, s, p->want_timing);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (rc != FRANK_OK) { if (g) cudaGraphDestroy(g); return rc; }
@@ -538,10 +554,8 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   ALLOC(t, nb * bm * bm * ts); p->WL = t;
   ALLOC(t, nb * bm * bm * ts); p->WU = t;
   ALLOC(p->getrf_scratch, bm * bm + 32 * bm);
-  ALLOC(p->dscratch, (int64_t)p->grid_dense * p->dstride);
-  if (p->nlr > 0)
-    ALLOC(p->rscratch, (int64_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
-                           p->rstride);
+  // dscratch / rscratch are allocated at the first factorization (ensure_scratch),
+  // so frank_blr_set_grid can size them for batched use first.
   ALLOC(t, p->n * 8 * ts); p->z = t;
   ALLOC(t, bm * 8 * ts); p->stmp = t;
   ALLOC(t, (int64_t)nb * bm * 8 * ts); p->sctmp = t;
@@ -995,6 +1009,16 @@ void free_batch(frank_batch* B) {
 }
 }  // namespace
 
+extern "C" int frank_blr_set_timing(frank_blr* p, int on) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  if (p->want_timing != (on != 0)) {
+    p->want_timing = on != 0;
+    if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
+    if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  }
+  return FRANK_OK;
+}
+
 extern "C" int frank_blr_set_grid(frank_blr* p, int ctas) {
   if (!p || ctas < 1) return fail(FRANK_ERR_INVALID, "bad grid");
   cudaDeviceSynchronize();
@@ -1004,10 +1028,6 @@ extern "C" int frank_blr_set_grid(frank_blr* p, int ctas) {
   p->grid_dense = std::max(1, std::min({nb * nb, 2 * p->sm_count, ctas}));
   if (p->rscratch) { cudaFree(p->rscratch); p->rscratch = nullptr; }
   if (p->dscratch) { cudaFree(p->dscratch); p->dscratch = nullptr; }
-  CUDA_TRY(dalloc(&p->dscratch, (size_t)p->grid_dense * p->dstride));
-  if (p->nlr > 0)
-    CUDA_TRY(dalloc(&p->rscratch, (size_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
-                                      p->rstride));
   if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
   if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
   p->factored = false;
@@ -1044,12 +1064,16 @@ namespace {
 template <typename T>
 int batch_capture(frank_batch* B) {
   cudaStream_t s = B->stream;
+  for (frank_blr* p : B->plans) {
+    int rc0 = ensure_scratch(p);
+    if (rc0) return rc0;
+  }
   CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int rc = FRANK_OK;
   cudaError_t e = cudaEventRecord(B->fork, s);
   for (size_t k = 0; rc == FRANK_OK && e == cudaSuccess && k < B->plans.size(); ++k) {
     e = cudaStreamWaitEvent(B->streams[k], B->fork, 0);
-    if (e == cudaSuccess) rc = enqueue_factor<T>(B->plans[k], B->streams[k]);
+    if (e == cudaSuccess) rc = enqueue_factor<T>(B->plans[k], B->streams[k], false);
     if (rc == FRANK_OK && e == cudaSuccess) e = cudaEventRecord(B->join[k], B->streams[k]);
     if (rc == FRANK_OK && e == cudaSuccess) e = cudaStreamWaitEvent(s, B->join[k], 0);
   }

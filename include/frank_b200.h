@@ -219,8 +219,14 @@ int frank_batch_refine_device(frank_batch* batch, const double* const* d_b, int6
 int frank_blr_stats(const frank_blr* plan, int64_t* launches, int64_t* recompressions,
                     int64_t* max_rank_seen, int64_t* rank_overflows);
 
+/* Record CUDA events around each launch class inside the factorization graph
+ * (on = 1) for frank_blr_kernel_times; off by default because event-record
+ * nodes serialise the graph's concurrent branches (the lookahead getrf). */
+int frank_blr_set_timing(frank_blr* plan, int on);
+
 /* Device time (ms, CUDA events recorded around each launch inside the
- * factorization graph) and algorithmic FLOPs of the last getrf, per kernel
+ * factorization graph when timing is on; zeros otherwise) and algorithmic
+ * FLOPs of the last getrf, per kernel
  * class: [0] leaf getrf + inverses, [1] panel trsm, [2] dense-target updates,
  * [3] LowRank recompression.  The FLOPs count the reference's call sequence
  * with the LAWN 41 operation counts (no reference counterpart; reporting). */
