@@ -56,7 +56,7 @@ struct frank_blr {
   // working copy (T)
   void *Wd = nullptr, *Wu = nullptr, *Ws = nullptr, *Wv = nullptr;
   // factor workspace
-  int *perm = nullptr, *ipiv = nullptr, *err = nullptr;
+  int *perm = nullptr, *ipiv = nullptr, *err = nullptr, *work = nullptr;
   void *Linv = nullptr, *Uinv = nullptr, *WL = nullptr, *WU = nullptr;
   double *getrf_scratch = nullptr, *dscratch = nullptr, *rscratch = nullptr;
   int64_t dstride = 0, rstride = 0;
@@ -126,7 +126,7 @@ FactorWs<T> factor_ws(frank_blr* p) {
   w.getrf_scratch = p->getrf_scratch;
   w.dscratch = p->dscratch; w.dscratch_stride = p->dstride;
   w.rscratch = p->rscratch; w.rscratch_stride = p->rstride;
-  w.err = p->err; w.flops = p->flops; w.fixed_rank = p->fixed_rank; w.eps = p->eps;
+  w.err = p->err; w.work = p->work; w.flops = p->flops; w.fixed_rank = p->fixed_rank; w.eps = p->eps;
   return w;
 }
 
@@ -173,6 +173,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   ++launches;
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
+  CUDA_TRY(cudaMemsetAsync(p->work, 0, 2 * p->nb * sizeof(int), s));
   CUDA_TRY(cudaEventRecord(p->fork, s));
   CUDA_TRY(cudaStreamWaitEvent(s2, p->fork, 0));
   auto getrf_on_aux = [&](int step) -> int {
@@ -208,16 +209,16 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
         // mixed path: Gram-based recompression of every low-rank x low-rank
         // update; the Householder kernel takes any target with a dense operand
         k_recompress_gram<T><<<std::min(mm, p->grid_gram), GRAM_THREADS, GRAM_SMEM_BYTES, s>>>(
-            W, ws, i, p->smax, p->core_scale, p->gram_tol);
+            W, ws, i, p->smax, p->core_scale, p->gram_tol, p->work + i);
         ++launches;
         if (p->dense_offdiag) {
           k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-              W, ws, i, p->smax, p->core_method, p->core_scale, 1);
+              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i);
           ++launches;
         }
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-            W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0);
+            W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0, p->work + i);
         ++launches;
       }
     }
@@ -419,7 +420,7 @@ void free_plan(frank_blr* p) {
   if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
   if (p->graph) cudaGraphDestroy(p->graph);
   void* ptrs[] = {p->d_off, p->d_dslot, p->d_lslot, p->d_rankH, p->d_rankW, p->Hd, p->Hu, p->Hs, p->Hv,
-                  p->Wd, p->Wu, p->Ws, p->Wv, p->perm, p->ipiv, p->err, p->Linv, p->Uinv, p->WL, p->WU,
+                  p->Wd, p->Wu, p->Ws, p->Wv, p->perm, p->ipiv, p->err, p->work, p->Linv, p->Uinv, p->WL, p->WU,
                   p->getrf_scratch, p->dscratch, p->rscratch, p->z, p->stmp, p->sctmp, p->part, p->vtmp, p->nrm};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->flops) cudaFree(p->flops);
@@ -548,6 +549,7 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   ALLOC(p->perm, nb * bm);
   ALLOC(p->ipiv, nb * bm);
   ALLOC(p->err, ERR_SLOTS);
+  ALLOC(p->work, 2 * nb);
   ALLOC(p->flops, FLOP_SLOTS);
   ALLOC(t, nb * bm * bm * ts); p->Linv = t;
   ALLOC(t, nb * bm * bm * ts); p->Uinv = t;

@@ -67,6 +67,7 @@ struct FactorWs {
   double* rscratch;       // recompression scratch, per CTA slot
   int64_t rscratch_stride;
   int* err;
+  int* work;                  // [nb] per-step work counters of the recompression
   unsigned long long* flops;  // [FLOP_SLOTS]
   int fixed_rank;
   double eps;
@@ -379,6 +380,25 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel(BlrView<T> A, FactorWs<
   }
 }
 
+// Task t (0 <= t < m*(m-1)) of step i's off-diagonal targets, ordered by
+// band d = |ic - k| = 1, 2, ... (the near-diagonal targets carry the largest
+// ranks, so they are handed out first), within a band by row.
+FRANK_D void band_task(int m, int t, int& a, int& c) {
+  int d = 1;
+  while (t >= 2 * (m - d)) { t -= 2 * (m - d); ++d; }
+  const int half = m - d;
+  if (t < half) { a = t + d; c = t; } else { a = t - half; c = t - half + d; }
+}
+
+// Next task of the step for this CTA (dynamic scheduling through an atomic
+// counter; all threads receive it).
+FRANK_D int next_task(int* counter, int* slot) {
+  __syncthreads();
+  if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+  __syncthreads();
+  return *slot;
+}
+
 // Operands of the update of target (ic, k) at step i:
 //   update = - XL * (WL^T WU) * YR^T,
 // XL = U(ic,i) (bc x p) or dense A(ic,i) (bc x bi, WL = I),
@@ -534,7 +554,7 @@ FRANK_HD RecompLayout recomp_layout(int bmax, int smax) {
 template <typename T>
 __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
                                                                int core_method, double core_scale,
-                                                               int only_dense_operands) {
+                                                               int only_dense_operands, int* counter) {
   extern __shared__ double dsm[];
   double* gsm = dsm;
   double* region = dsm + RECOMP_GSM;
@@ -570,8 +590,12 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
   int* jinv = reinterpret_cast<int*>(base + L.ji);
   double* smP = region;
   double* smT = region + (int64_t)A.bmax * QRB;
-  for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
-    const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
+  __shared__ int s_task;
+  const int ntask = m * (m - 1);
+  for (int tsk = next_task(counter, &s_task); tsk < ntask; tsk = next_task(counter, &s_task)) {
+    int a_, c_;
+    band_task(m, tsk, a_, c_);
+    const int ic = i + 1 + a_, k = i + 1 + c_;
     if (!A.is_lr(ic, k)) continue;
     if (only_dense_operands && A.is_lr(ic, i) && A.is_lr(i, k)) continue;
     const int blk = ic * A.nb + k;
@@ -816,7 +840,7 @@ FRANK_HD GramLayout gram_layout(int bmax, int smax) {
 
 template <typename T>
 __global__ void __launch_bounds__(GRAM_THREADS) k_recompress_gram(BlrView<T> A, FactorWs<T> ws, int i, int smax,
-                                                                  double core_scale, double gram_tol) {
+                                                                  double core_scale, double gram_tol, int* counter) {
   extern __shared__ double region[];
   __shared__ double gsm[2 * 16 * 64];
   __shared__ double red[32];
@@ -828,8 +852,12 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_recompress_gram(BlrView<T> A, 
   const int bi = A.bs(i);
   const GramLayout L = gram_layout(A.bmax, smax);
   double* base = ws.rscratch + (int64_t)blockIdx.x * ws.rscratch_stride;
-  for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
-    const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
+  __shared__ int s_task;
+  const int ntask = m * (m - 1);
+  for (int tsk = next_task(counter, &s_task); tsk < ntask; tsk = next_task(counter, &s_task)) {
+    int a_, c_;
+    band_task(m, tsk, a_, c_);
+    const int ic = i + 1 + a_, k = i + 1 + c_;
     if (!A.is_lr(ic, k) || !A.is_lr(ic, i) || !A.is_lr(i, k)) continue;
     const int blk = ic * A.nb + k;
     const int bc = A.bs(ic), bk = A.bs(k);
