@@ -100,6 +100,17 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(values, world, device="cpu"):
+    """Element-wise max over the ranks of a list of per-step times (the
+    replicas-only multi-GPU reduction: no data-path collective, only this)."""
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.cpu().tolist()
+
+
 def fp64_gemm_peak(torch):
     """Measured cuBLAS FP64 GEMM throughput (TFLOP/s), the FP64 roofline denominator."""
     n = 8192
@@ -189,15 +200,9 @@ def run_ours(args, rank, world):
 
     peak64 = fp64_gemm_peak(torch)
     # max over ranks of the per-step times
-    def agg(v):
-        t = torch.tensor(v, dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.cpu().tolist()
-
     for prec in arms:
-        arms[prec]["times"] = agg(arms[prec]["times"])
-        arms[prec]["e2e"] = agg(arms[prec]["e2e"])
+        arms[prec]["times"] = max_over_ranks(arms[prec]["times"], world, "cuda")
+        arms[prec]["e2e"] = max_over_ranks(arms[prec]["e2e"], world, "cuda")
     return arms, peak64
 
 

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -671,7 +672,8 @@ int frank_blr_build_kernel(frank_blr* p, int kernel, const double* points, int d
                            double eps, void* stream) {
   if (!p || !points) return fail(FRANK_ERR_INVALID, "null argument");
   if (kernel < 0 || kernel > 3 || dim < 1 || dim > 3) return fail(FRANK_ERR_INVALID, "bad kernel or dim");
-  if (eps <= 0.0) return fail(FRANK_ERR_UNSUPPORTED, "on-device construction needs eps > 0");
+  if (eps <= 0.0 && p->fixed_rank <= 0)
+    return fail(FRANK_ERR_UNSUPPORTED, "on-device construction needs eps > 0 or a fixed-rank plan");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* dx = nullptr;
   CUDA_TRY(cudaMalloc(&dx, sizeof(double) * dim * p->n));
@@ -694,7 +696,43 @@ int frank_blr_build_kernel(frank_blr* p, int kernel, const double* points, int d
   BlrView<double> H = h_view(p);
   if (!dl.empty()) k_build_dense<<<(int)std::min<size_t>(dl.size(), 4096), 256, 0, s>>>(H, K, d_dl, (int)dl.size());
   int rc = FRANK_OK;
-  if (!ll.empty()) {
+  if (!ll.empty() && eps <= 0.0) {
+    // fixed rank: LowRank(Dense, rank) -> rsvd with sample min(rank + 5, m, n)
+    // and the reference's Omega (random_uniform, functions.cpp:52-66)
+    const int64_t bm = p->bmax;
+    const int last = p->off_h[p->nb] - p->off_h[p->nb - 1];
+    const int psamp = std::min<int>(p->fixed_rank + 5, std::min<int>(bm, last));
+    if (p->fixed_rank + 5 > last && last != bm) {
+      cudaFree(dx);
+      return fail(FRANK_ERR_UNSUPPORTED, "fixed-rank construction with a short last block below rank + 5");
+    }
+    auto omega = [&](int ncols) {
+      std::mt19937 gen;
+      gen.seed(0);
+      std::uniform_real_distribution<double> dist(0.0, 1.0);
+      std::vector<double> om((size_t)ncols * psamp);
+      for (auto& v : om) v = dist(gen);
+      return om;
+    };
+    const std::vector<double> of = omega((int)bm), ol = omega(last);
+    double *d_of = nullptr, *d_ol = nullptr;
+    CUDA_TRY(cudaMalloc(&d_of, sizeof(double) * of.size()));
+    CUDA_TRY(cudaMalloc(&d_ol, sizeof(double) * ol.size()));
+    CUDA_TRY(cudaMemcpy(d_of, of.data(), sizeof(double) * of.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d_ol, ol.data(), sizeof(double) * ol.size(), cudaMemcpyHostToDevice));
+    const int64_t stride = bm * bm + 2 * bm * psamp + (bm + psamp) * psamp + 4 * psamp + 64;
+    const int grid = (int)std::min<size_t>(ll.size(), (size_t)2 * p->sm_count);
+    double* scratch = nullptr;
+    CUDA_TRY(cudaMalloc(&scratch, sizeof(double) * stride * grid));
+    CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
+    k_build_lowrank_rsvd<<<grid, BUILD_THREADS, 0, s>>>(H, K, d_ll, (int)ll.size(), p->fixed_rank, psamp, d_of, d_ol,
+                                                        stride, scratch, p->err);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaMemcpy(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(scratch); cudaFree(d_of); cudaFree(d_ol);
+    if (p->err_h[ERR_RANK_OVERFLOW]) rc = fail(FRANK_ERR_RANK_OVERFLOW, "the fixed rank exceeds max_rank");
+  } else if (!ll.empty()) {
     const int64_t bm = p->bmax;
     const int64_t stride = 3 * bm * bm + 6 * bm;
     const int grid = (int)std::min<size_t>(ll.size(), (size_t)2 * p->sm_count);

@@ -1720,4 +1720,100 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_build_lowrank(BlrView<double>
   }
 }
 
+// Fixed-rank compression of the admissible blocks by randomized SVD
+// (classes/low_rank.cpp:40-48 -> operations/randomized/rsvd.cpp:17-29):
+// Y = A Omega with the reference's Omega (uniform [0,1), std::mt19937 seeded
+// 0, row-major n x p, the same matrix for every block of that width; passed
+// in by the host), Q = qr(Y), B = Q^T A, thin SVD of B by one-sided Jacobi
+// on B^T with the rotations accumulated in p appended rows, U = Q Ub, then
+// truncation to `rank`.  One CTA per block, FP64 scratch slot per CTA:
+// A (b x b), Y / Q (b x p), Bt (b + p) x p, small vectors.
+__global__ void __launch_bounds__(BUILD_THREADS) k_build_lowrank_rsvd(BlrView<double> H, KernelDesc K,
+                                                                      const int* blocks, int nblocks, int rank,
+                                                                      int p, const double* omega_full,
+                                                                      const double* omega_last, int64_t stride,
+                                                                      double* scratch, int* err) {
+  __shared__ double red[32];
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ int flag;
+  const int ld = H.bmax;
+  double* base = scratch + (int64_t)blockIdx.x * stride;
+  double* Am = base;                               // m x n
+  double* Ym = Am + (int64_t)ld * ld;              // m x p (QR in place)
+  double* Qm = Ym + (int64_t)ld * p;               // m x p explicit Q
+  double* Bt = Qm + (int64_t)ld * p;               // (n + p) x p
+  double* tau = Bt + (int64_t)(ld + p) * p;        // p
+  double* sig = tau + p;                           // p
+  int* ord = reinterpret_cast<int*>(sig + p);      // p
+  for (int t = blockIdx.x; t < nblocks; t += gridDim.x) {
+    const int blk = blocks[t];
+    const int i = blk / H.nb, j = blk % H.nb;
+    const int m = H.bs(i), n = H.bs(j);
+    const double* Om = (n == ld) ? omega_full : omega_last;   // n x p row-major
+    for (int64_t e = threadIdx.x; e < (int64_t)m * n; e += blockDim.x) {
+      const int r = e % m, c = e / m;
+      Am[r + (int64_t)c * m] = kernel_eval(K, H.off[i] + r, H.off[j] + c);
+    }
+    __syncthreads();
+    // Y = A Omega: Omega row-major n x p == column-major p x n, used transposed
+    cta_gemm<double, BUILD_THREADS>(m, p, n, 1.0, Am, m, false, Om, p, true, 0.0, Ym, m, gsm);
+    cta_householder_qr(m, p, Ym, m, tau, red);
+    for (int64_t e = threadIdx.x; e < (int64_t)m * p; e += blockDim.x) {
+      const int r = e % m, c = e / m;
+      Qm[e] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    cta_apply_q(m, p, Ym, m, tau, p, Qm, (int64_t)m);
+    // Bt (n x p) = (Q^T A)^T = A^T Q; identity appended below (p x p)
+    cta_gemm<double, BUILD_THREADS>(n, p, m, 1.0, Am, m, true, Qm, m, false, 0.0, Bt, n + p, gsm);
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
+      const int r = e % p, c = e / p;
+      Bt[(n + r) + (int64_t)c * (n + p)] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const int sweeps = cta_jacobi_columns(n, p, Bt, n + p, 60, &flag, n + p);
+    if (sweeps < 0 && threadIdx.x == 0) atomicAdd(err + ERR_JACOBI, 1);
+    // Bt columns: W Sigma (top n rows), Z (bottom p rows); B = Z Sigma W^T
+    for (int c = threadIdx.x >> 5; c < p; c += blockDim.x >> 5) {
+      double sacc = 0.0;
+      for (int r = threadIdx.x & 31; r < n; r += 32) sacc += Bt[r + (int64_t)c * (n + p)] * Bt[r + (int64_t)c * (n + p)];
+      sacc = warp_sum(sacc);
+      if ((threadIdx.x & 31) == 0) sig[c] = sqrt(sacc);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < p; c += blockDim.x) {
+      const double v = sig[c];
+      int pos = 0;
+      for (int d = 0; d < p; ++d) pos += (sig[d] > v) || (sig[d] == v && d < c);
+      ord[pos] = c;
+    }
+    __syncthreads();
+    const int rk = min(rank, H.kcap);
+    if (rank > H.kcap && threadIdx.x == 0) atomicAdd(err + ERR_RANK_OVERFLOW, 1);
+    double* Ud = H.u(i, j);
+    double* Vd = H.vt(i, j);
+    double* Sd = H.s(i, j);
+    // U = Q Z[:, ord] (m x rk); Vt = W[:, ord] (n x rk) normalised; S = diag
+    for (int64_t e = threadIdx.x; e < (int64_t)m * rk; e += blockDim.x) {
+      const int r = e % m, c = e / m;
+      const int src = ord[c];
+      double acc = 0.0;
+      for (int t = 0; t < p; ++t) acc += Qm[r + (int64_t)t * m] * Bt[(n + t) + (int64_t)src * (n + p)];
+      Ud[r + (int64_t)c * ld] = acc;
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)n * rk; e += blockDim.x) {
+      const int r = e % n, c = e / n;
+      const int src = ord[c];
+      const double sv = sig[src];
+      Vd[r + (int64_t)c * ld] = sv > 0.0 ? Bt[r + (int64_t)src * (n + p)] / sv : 0.0;
+    }
+    for (int64_t e = threadIdx.x; e < (int64_t)rk * rk; e += blockDim.x) {
+      const int r = e % rk, c = e / rk;
+      Sd[r + (int64_t)c * H.kcap] = (r == c) ? sig[ord[c]] : 0.0;
+    }
+    if (threadIdx.x == 0) H.rank[blk] = rk;
+    __syncthreads();
+  }
+}
+
 }  // namespace frank

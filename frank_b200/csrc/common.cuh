@@ -249,7 +249,10 @@ FRANK_D void cta_apply_q(int m, int k, const double* V, int64_t ldv, const doubl
 // "Jacobi's method is more accurate than QR", 1992).  Returns the number of
 // sweeps, or -1 if max_sweeps was reached without convergence.
 // ---------------------------------------------------------------------------
-FRANK_D int cta_jacobi_columns(int m, int n, double* G, int64_t ldg, int max_sweeps, int* flag) {
+FRANK_D int cta_jacobi_columns(int m, int n, double* G, int64_t ldg, int max_sweeps, int* flag, int m_rot = -1) {
+  // rotation angles from rows [0, m); rotations applied to rows [0, m_rot)
+  // (m_rot > m accumulates the right singular vectors in appended rows)
+  if (m_rot < m) m_rot = m;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int N2 = n + (n & 1);
   const double tol = (double)(m > 1 ? m : 1) * 2.220446049250313e-16;
@@ -278,7 +281,7 @@ FRANK_D int cta_jacobi_columns(int m, int n, double* G, int64_t ldg, int max_swe
         const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
         const double c = 1.0 / sqrt(1.0 + t * t);
         const double s = c * t;
-        for (int i = lane; i < m; i += 32) {
+        for (int i = lane; i < m_rot; i += 32) {
           const double x = gp[i], y = gq[i];
           gp[i] = c * x - s * y;
           gq[i] = s * x + c * y;

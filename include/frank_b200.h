@@ -104,7 +104,10 @@ int frank_blr_set_lowrank(frank_blr* plan, int i, int j, int rank,
  * reference's params[d][i], functions.h:34-38): diagonal and inadmissible
  * blocks dense, admissible blocks compressed by truncated column-pivoted QR
  * + RQ (LowRank(Dense, eps), low_rank.cpp:50-59 with geqp3.cpp:71-192) when
- * eps > 0.  Which blocks are low rank follows the plan's admissibility.
+ * eps > 0, or by randomized SVD to the plan's fixed rank when eps = 0
+ * (LowRank(Dense, rank), low_rank.cpp:40-48 -> rsvd.cpp:17-29, with the
+ * reference's Omega: uniform [0,1) from std::mt19937 seeded 0, functions.cpp:52-66).
+ * Which blocks are low rank follows the plan's admissibility.
  * kparams: kernel parameters (see FRANK_KERNEL_*), may be NULL.  Replaces
  * Hierarchical(kernel, params, n, n, nleaf, eps, admis, nb, nb)
  * (classes/hierarchical.cpp:89-109) for one level. */

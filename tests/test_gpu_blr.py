@@ -159,3 +159,31 @@ def test_mixed_factor_error_matches_oracle(gpu_lib, feps, lra):
     M.getrf()
     gpu_ferr = _factor_error(A_dense, M)
     assert gpu_ferr <= FACTOR * ref_ferr + 1e-6, (gpu_ferr, ref_ferr)
+
+
+def test_device_fixed_rank_construction_matches_oracle(gpu_lib):
+    """frank_blr_build_kernel on a fixed-rank plan: randomized SVD with the
+    reference's Omega (std::mt19937(0) uniform draws) equals the oracle's
+    LowRank(Dense, 16) blocks (rsvd.cpp:17-29) to roundoff, on the N=2048
+    Laplace-1D workload; the factor + solve then matches the oracle's."""
+    from frank_b200 import BLRMatrix
+    n, nb, rank = 2048, 8, 16
+    x = np.array([fo.get_sorted_random_vector(n)])
+    A = fo.build_hierarchical(fo.laplacend, x, n, 256, nb, rank=rank)
+    M = BLRMatrix(n, nb, fixed_rank=rank)
+    M.build_kernel("laplace", x, 0.0)
+    for i in range(nb):
+        for j in range(nb):
+            ref = fo.to_dense(A[i, j])
+            got = M.block_dense(i, j)
+            assert np.linalg.norm(got - ref) <= 1e-10 * np.linalg.norm(ref), (i, j)
+            if i != j:
+                assert M.rank(i, j) == rank
+    rng = np.random.default_rng(1)
+    bv = rng.standard_normal((n, 1))
+    L, U = fo.getrf(fo.deep_copy(A))
+    xo = fo.solve(L, U, bv)
+    M.getrf()
+    xg = M.solve(bv)
+    xd = np.linalg.solve(fo.to_dense(A), bv)
+    assert np.linalg.norm(xg - xd) <= FACTOR * np.linalg.norm(xo - xd) + 1e-13 * np.linalg.norm(xd)
