@@ -189,6 +189,15 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   ++launches;
   for (int i = 0; i < p->nb; ++i) {
     CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[i], 0));
+    {
+      // explicit inverses of step i's factors, all column blocks in parallel
+      const int cw = trinv_width(p->bmax);
+      const int nblk = (int)((p->off_h[i + 1] - p->off_h[i] + cw - 1) / cw);
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_TRINV, 0), s, cudaEventRecordExternal));
+      k_trinv<T><<<2 * nblk, TRINV_THREADS, (size_t)p->bmax * cw * sizeof(double), s>>>(W, ws, i, cw);
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_TRINV, 1), s, cudaEventRecordExternal));
+      ++launches;
+    }
     const int m = p->nb - i - 1;
     if (m == 0) break;
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
@@ -237,7 +246,7 @@ int collect_times(frank_blr* p) {
   if (!p->timed) return FRANK_OK;
   for (int i = 0; i < p->nb; ++i)
     for (int c = 0; c < FLOP_SLOTS; ++c) {
-      if (i == p->nb - 1 && c != FLOP_GETRF) continue;
+      if (i == p->nb - 1 && c != FLOP_GETRF && c != FLOP_TRINV) continue;
       float ms = 0.f;
       cudaError_t e = cudaEventElapsedTime(&ms, ev_at(p, i, c, 0), ev_at(p, i, c, 1));
       if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("event timing: ") + cudaGetErrorString(e));
@@ -605,6 +614,8 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
   cudaFuncSetAttribute(k_solve_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shd);
   cudaFuncSetAttribute(k_solve_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shd);
+  cudaFuncSetAttribute(k_trinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRINV_SMEM_MAX);
+  cudaFuncSetAttribute(k_trinv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRINV_SMEM_MAX);
   cudaFuncSetAttribute(k_recompress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, GRAM_SMEM_BYTES);
@@ -955,8 +966,9 @@ int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int6
 
 int frank_blr_kernel_times(const frank_blr* p, double* ms, double* flops) {
   if (!p) return fail(FRANK_ERR_INVALID, "null plan");
-  for (int c = 0; c < FLOP_SLOTS; ++c) {
-    if (ms) ms[c] = p->class_ms[c];
+  // four reported classes; the inverse kernel's time belongs to class 0
+  for (int c = 0; c < FLOP_TRINV; ++c) {
+    if (ms) ms[c] = p->class_ms[c] + (c == FLOP_GETRF ? p->class_ms[FLOP_TRINV] : 0.0);
     if (flops) flops[c] = (double)p->flops_h[c];
   }
   return FRANK_OK;
@@ -1210,6 +1222,13 @@ extern "C" int frank_batch_refine_device(frank_batch* B, const double* const* d_
 
 #ifdef FRANK_PHASE_TIMING
 // Read and clear the recompression phase counters (timing builds only).
+extern "C" int frank_debug_getrf_cycles(unsigned long long* c8) {
+  CUDA_TRY(cudaMemcpyFromSymbol(c8, g_getrf_cycles, sizeof(unsigned long long) * 8));
+  unsigned long long z[8] = {0};
+  CUDA_TRY(cudaMemcpyToSymbol(g_getrf_cycles, z, sizeof(z)));
+  return FRANK_OK;
+}
+
 extern "C" int frank_debug_phase_cycles(unsigned long long* cycles16, unsigned long long* count2) {
   CUDA_TRY(cudaMemcpyFromSymbol(cycles16, g_phase_cycles, sizeof(unsigned long long) * 16));
   CUDA_TRY(cudaMemcpyFromSymbol(count2, g_phase_count, sizeof(unsigned long long) * 2));
@@ -1226,7 +1245,7 @@ extern "C" int frank_debug_phase_cycles(unsigned long long* cycles16, unsigned l
 // For callers that cannot call cudaMalloc (inside an allocator callback, on an
 // out-of-memory recovery path, under a pool that forbids growth).  All device
 // scratch comes from the file-scope array below: the block copy D, the FP64
-// work matrix of k_getrf, the explicit inverses k_getrf also forms, the pivot
+// work matrix of k_getrf, two reserved inverse-sized slots, the pivot
 // and permutation vectors, and the small geometry / status words.  Nothing in
 // this section changes the plan-based paths above.
 // ===========================================================================

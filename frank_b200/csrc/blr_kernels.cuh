@@ -35,6 +35,21 @@ struct BlrView {
 // Optional per-phase cycle counters of the recompression kernels (build with
 // -DFRANK_PHASE_TIMING; off by default).  Slots: [size class][phase].
 #ifdef FRANK_PHASE_TIMING
+__device__ unsigned long long g_getrf_cycles[8];
+#define GPHASE(k)                                                                           \
+  do {                                                                                      \
+    if (threadIdx.x == 0) {                                                                 \
+      const long long _t = clock64();                                                      \
+      atomicAdd(&g_getrf_cycles[(k)], (unsigned long long)(_t - _g_t0));                    \
+      _g_t0 = _t;                                                                           \
+    }                                                                                       \
+  } while (0)
+#define GPHASE_BEGIN() long long _g_t0 = clock64()
+#else
+#define GPHASE(k) do {} while (0)
+#define GPHASE_BEGIN() do {} while (0)
+#endif
+#ifdef FRANK_PHASE_TIMING
 __device__ unsigned long long g_phase_cycles[2][8];
 __device__ unsigned long long g_phase_count[2];
 #define PHASE_BEGIN() long long _ph_t0 = clock64(); int _ph_last = 0
@@ -153,45 +168,117 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
   int* perm = ws.perm + (int64_t)i * A.bmax;
   T* Li = ws.Linv + (int64_t)i * A.bmax * A.bmax;
   T* Ui = ws.Uinv + (int64_t)i * A.bmax * A.bmax;
+  GPHASE_BEGIN();
   for (int64_t e = threadIdx.x; e < (int64_t)b * b; e += blockDim.x) {
     const int r = e % b, c = e / b;
     Wm[r + (int64_t)c * b] = double(Dp[r + (int64_t)c * ldA]);
   }
   __syncthreads();
+  GPHASE(0);
   int first_zero = -1;
+  __shared__ double prow[32];          // pivot row of the panel, broadcast
+  __shared__ double xrow[32];          // row exchanged with the pivot row
   for (int jb = 0; jb < b; jb += 32) {
     const int jn = min(32, b - jb);
-    for (int j = jb; j < jb + jn; ++j) {
-      double best = -1.0;
-      int bi = -1;
-      for (int r = j + threadIdx.x; r < b; r += blockDim.x) {
-        const double a = fabs(Wm[r + (int64_t)j * b]);
-        if (a > best) { best = a; bi = r; }
+    if (b <= GETRF_THREADS) {
+      // Panel in registers: thread t owns row t (t >= jb) and its jn panel
+      // entries; a column step is an arg-max, a row exchange through shared
+      // memory and a rank-1 update, with no global traffic.
+      const int t = threadIdx.x;
+      const bool own = (t >= jb && t < b);
+      double a[32];
+#pragma unroll
+      for (int c = 0; c < 32; ++c) a[c] = (own && c < jn) ? Wm[t + (int64_t)(jb + c) * b] : 0.0;
+      for (int jj = 0; jj < jn; ++jj) {
+        const int j = jb + jj;
+        double v = -1.0;
+        int vi = -1;
+        if (t >= j && t < b) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) if (c == jj) v = fabs(a[c]);
+          vi = t;
+        }
+        double amax;
+        const int p = block_argmax_abs(v < 0.0 ? 0.0 : v, vi, red, redi, &amax);
+        if (threadIdx.x == 0) piv[j] = p;
+        if (amax == 0.0 && first_zero < 0) first_zero = j;
+        // the pivot row goes to row j, row j to row p
+        if (t == p) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) prow[c] = a[c];
+        }
+        if (t == j) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) xrow[c] = a[c];
+        }
+        __syncthreads();
+        if (t == j) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) a[c] = prow[c];
+        } else if (t == p) {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) a[c] = xrow[c];
+        }
+        if (t > j && t < b && amax != 0.0) {
+          const double rcp = 1.0 / prow[jj];
+          double l = 0.0;
+#pragma unroll
+          for (int c = 0; c < 32; ++c) if (c == jj) { a[c] *= rcp; l = a[c]; }
+#pragma unroll
+          for (int c = 0; c < 32; ++c) if (c > jj) a[c] -= l * prow[c];
+        }
+        __syncthreads();
       }
-      double amax;
-      const int p = block_argmax_abs(best < 0.0 ? 0.0 : best, bi, red, redi, &amax);
-      if (threadIdx.x == 0) piv[j] = p;
-      if (amax == 0.0 && first_zero < 0) first_zero = j;
-      if (p != j && amax != 0.0) {
-        for (int c = threadIdx.x; c < b; c += blockDim.x) {
-          const double t = Wm[j + (int64_t)c * b];
-          Wm[j + (int64_t)c * b] = Wm[p + (int64_t)c * b];
-          Wm[p + (int64_t)c * b] = t;
+      if (own) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) if (c < jn) Wm[t + (int64_t)(jb + c) * b] = a[c];
+      }
+      __syncthreads();
+      // the panel's interchanges applied to the columns outside the panel
+      for (int c = threadIdx.x; c < b; c += blockDim.x) {
+        if (c >= jb && c < jb + jn) continue;
+        double* col = Wm + (int64_t)c * b;
+        for (int jj = 0; jj < jn; ++jj) {
+          const int j = jb + jj, p = piv[j];
+          if (p != j) { const double tmp = col[j]; col[j] = col[p]; col[p] = tmp; }
         }
       }
       __syncthreads();
-      if (amax != 0.0) {
-        const double rcp = 1.0 / Wm[j + (int64_t)j * b];
-        for (int r = j + 1 + threadIdx.x; r < b; r += blockDim.x) Wm[r + (int64_t)j * b] *= rcp;
+    } else {
+      // blocks larger than the thread count: column steps on the global copy
+      for (int j = jb; j < jb + jn; ++j) {
+        double best = -1.0;
+        int bi = -1;
+        for (int r = j + threadIdx.x; r < b; r += blockDim.x) {
+          const double av = fabs(Wm[r + (int64_t)j * b]);
+          if (av > best) { best = av; bi = r; }
+        }
+        double amax;
+        const int p = block_argmax_abs(best < 0.0 ? 0.0 : best, bi, red, redi, &amax);
+        if (threadIdx.x == 0) piv[j] = p;
+        if (amax == 0.0 && first_zero < 0) first_zero = j;
+        if (p != j && amax != 0.0) {
+          for (int c = threadIdx.x; c < b; c += blockDim.x) {
+            const double tt = Wm[j + (int64_t)c * b];
+            Wm[j + (int64_t)c * b] = Wm[p + (int64_t)c * b];
+            Wm[p + (int64_t)c * b] = tt;
+          }
+        }
+        __syncthreads();
+        if (amax != 0.0) {
+          const double rcp = 1.0 / Wm[j + (int64_t)j * b];
+          for (int r = j + 1 + threadIdx.x; r < b; r += blockDim.x) Wm[r + (int64_t)j * b] *= rcp;
+        }
+        __syncthreads();
+        const int nr = b - j - 1, nc = jb + jn - j - 1;
+        for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+          const int r = j + 1 + e % nr, c = j + 1 + e / nr;
+          Wm[r + (int64_t)c * b] -= Wm[r + (int64_t)j * b] * Wm[j + (int64_t)c * b];
+        }
+        __syncthreads();
       }
-      __syncthreads();
-      const int nr = b - j - 1, nc = jb + jn - j - 1;
-      for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
-        const int r = j + 1 + e % nr, c = j + 1 + e / nr;
-        Wm[r + (int64_t)c * b] -= Wm[r + (int64_t)j * b] * Wm[j + (int64_t)c * b];
-      }
-      __syncthreads();
     }
+    GPHASE(1);
     // U12 = L11^{-1} A12: invert the unit-lower 32x32 L11 into tri, then a
     // CTA GEMM into the scratch panel and back.
     const int ncr = b - jb - jn;
@@ -216,14 +303,16 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
       }
       __syncthreads();
     }
+    GPHASE(2);
     const int m2 = b - jb - jn;
     if (m2 > 0)
       cta_gemm<double, GETRF_THREADS>(m2, m2, jn, -1.0, Wm + (jb + jn) + (int64_t)jb * b, b, false,
                                       Wm + jb + (int64_t)(jb + jn) * b, b, false, 1.0,
                                       Wm + (jb + jn) + (int64_t)(jb + jn) * b, b, gsm);
   }
+  GPHASE(3);
   if (threadIdx.x == 0) {
-    atomicAdd(ws.flops + FLOP_GETRF, (unsigned long long)(4.0 / 3.0 * (double)b * b * b));
+    atomicAdd(ws.flops + FLOP_GETRF, (unsigned long long)(2.0 / 3.0 * (double)b * b * b));
     if (first_zero >= 0) atomicCAS(ws.err + ERR_SINGULAR_STEP, 0, i + 1);
     // permutation from the interchanges: (P B)[r] = B[perm[r]]
     for (int r = 0; r < b; ++r) perm[r] = r;
@@ -238,69 +327,96 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
     Dp[r + (int64_t)c * ldA] = T(Wm[r + (int64_t)c * b]);
   }
   __syncthreads();
-  // ---- Uinv = U^{-1}, by 32-column blocks from the left (dtrtri order):
-  //   X_jj = inv(U_jj);  X[0:jb, jb:jb+jn] = -(X[0:jb, 0:jb] U[0:jb, jb:jb+jn]) X_jj
-  for (int jb = 0; jb < b; jb += 32) {
-    const int jn = min(32, b - jb);
-    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
+  GPHASE(5);
+}
+
+// ---------------------------------------------------------------------------
+// K1': explicit inverses of the factors of diagonal block i, Uinv = U^{-1} and
+// Linv = L^{-1} (L unit lower), in column blocks of width cw: CTA q < nblk
+// forms column block q of Uinv, CTA nblk + q column block q of Linv.  The
+// column blocks are independent, so all 2 * nblk CTAs run at once.  A CTA
+// keeps its b x cw block X of the inverse in shared memory (FP64) and sweeps
+// the 32-row blocks in substitution order (upper: from the diagonal up to
+// row 0; lower: from the diagonal down): acc = E - T(rb, solved) X(solved)
+// by a CTA GEMM, then X(rb) = T(rb, rb)^{-1} acc by warp substitution (one
+// warp per column, lane = row, the solved value broadcast by shuffle).  The
+// packed LU is read from the block (precision T).  (LAPACK dtrtri forms the
+// same inverse, by column blocks in sequence.)
+// ---------------------------------------------------------------------------
+constexpr int TRINV_THREADS = 256;
+
+// Column-block width for block order bmax: X (bmax x cw doubles) must fit in
+// shared memory beside the static arrays.
+inline int trinv_width(int bmax) { return bmax <= 640 ? 32 : 16; }
+constexpr int TRINV_SMEM_MAX = 640 * 32 * (int)sizeof(double);   // covers 1024 x 16 too
+
+template <typename T>
+__global__ void __launch_bounds__(TRINV_THREADS) k_trinv(BlrView<T> A, FactorWs<T> ws, int i, int cw) {
+  extern __shared__ double X[];        // b x cw (ld b), rows indexed absolutely
+  __shared__ double tri[32 * 33];
+  __shared__ double acc[32 * 32];
+  __shared__ double gsm[2 * 16 * 64];
+  const int b = A.bs(i), ld = A.bmax;
+  const T* LU = A.dense(i, i);
+  const int nblk = (b + cw - 1) / cw;
+  const bool upper = (int)blockIdx.x < nblk;
+  const int cb = upper ? blockIdx.x : blockIdx.x - nblk;
+  const int c0 = cb * cw, cn = min(cw, b - c0);
+  if (c0 >= b) return;
+  T* out = (upper ? ws.Uinv : ws.Linv) + (int64_t)i * ld * ld;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int nrb = (b + 31) / 32;
+  // upper: rows at or above the last diagonal row c0+cn-1; lower: from c0 down
+  const int rb_first = upper ? (c0 + cn - 1) / 32 : c0 / 32;
+  const int rb_last = upper ? 0 : nrb - 1;
+  const int rb_step = upper ? -1 : 1;
+  for (int rb = rb_first;; rb += rb_step) {
+    const int r0 = rb * 32, rn = min(32, b - r0);
+    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+      const int r = e % 32, c = e / 32;
+      acc[e] = (r < rn && c < cn && r0 + r == c0 + c) ? 1.0 : 0.0;
+      tri[r + c * 33] = (r < rn && c < rn) ? double(LU[(r0 + r) + (int64_t)(r0 + c) * ld]) : 0.0;
+    }
     __syncthreads();
-    if (threadIdx.x < jn) {
-      const int c = threadIdx.x;
-      tri[c + c * 33] = 1.0 / Wm[(jb + c) + (int64_t)(jb + c) * b];
-      for (int r = c - 1; r >= 0; --r) {
-        double s = 0.0;
-        for (int t = r + 1; t <= c; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
-        tri[r + c * 33] = -s / Wm[(jb + r) + (int64_t)(jb + r) * b];
+    if (upper) {
+      const int k0 = r0 + rn, kn = c0 + cn - k0;   // solved rows of X below this block
+      if (kn > 0)
+        cta_gemm<double, TRINV_THREADS>(rn, cn, kn, -1.0, LU + r0 + (int64_t)k0 * ld, ld, false, X + k0, b, false,
+                                        1.0, acc, 32, gsm);
+    } else {
+      const int k0 = c0, kn = r0 - c0;              // solved rows of X above this block
+      if (kn > 0)
+        cta_gemm<double, TRINV_THREADS>(rn, cn, kn, -1.0, LU + r0 + (int64_t)k0 * ld, ld, false, X + k0, b, false,
+                                        1.0, acc, 32, gsm);
+    }
+    __syncthreads();
+    for (int c = wid; c < cn; c += nw) {
+      double v = lane < rn ? acc[lane + c * 32] : 0.0;
+      if (upper) {
+        for (int t = rn - 1; t >= 0; --t) {
+          const double xt = __shfl_sync(0xffffffffu, v, t) / tri[t + t * 33];
+          if (lane == t) v = xt;
+          else if (lane < t) v -= tri[lane + t * 33] * xt;
+        }
+      } else {
+        for (int t = 0; t < rn; ++t) {
+          const double xt = __shfl_sync(0xffffffffu, v, t);
+          if (lane > t) v -= tri[lane + t * 33] * xt;
+        }
       }
+      if (lane < rn) X[r0 + lane + (int64_t)c * b] = v;
     }
     __syncthreads();
-    if (jb > 0) {
-      // Gp (jb x jn) = X[0:jb, 0:jb] U[0:jb, jb:jb+jn]   (U read from the upper part of Wm)
-      cta_gemm<double, GETRF_THREADS>(jb, jn, jb, 1.0, Ui, ldA, false, Wm + (int64_t)jb * b, b, false, 0.0, Gp, jb,
-                                      gsm);
-      // X[0:jb, jb:jb+jn] = -Gp X_jj
-      cta_gemm<double, GETRF_THREADS>(jb, jn, jn, -1.0, Gp, jb, false, tri, 33, false, 0.0, Ui + (int64_t)jb * ldA,
-                                      ldA, gsm);
-    }
-    for (int e = threadIdx.x; e < (b - jb) * jn; e += blockDim.x) {
-      const int r = jb + e % (b - jb), c = e / (b - jb);
-      Ui[r + (int64_t)(jb + c) * ldA] = T((r < jb + jn) ? tri[(r - jb) + c * 33] : 0.0);
-    }
-    __syncthreads();
+    if (rb == rb_last) break;
   }
-  // ---- Linv = L^{-1} (unit lower), by 32-column blocks from the bottom:
-  //   X_jj = inv(L_jj);  X[jb+jn:b, jb:jb+jn] = -(X[jb+jn:b, jb+jn:b] L[jb+jn:b, jb:jb+jn]) X_jj
-  const int nblk = (b + 31) / 32;
-  for (int blk = nblk - 1; blk >= 0; --blk) {
-    const int jb = blk * 32;
-    const int jn = min(32, b - jb);
-    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
-    __syncthreads();
-    if (threadIdx.x < jn) {
-      const int c = threadIdx.x;
-      tri[c + c * 33] = 1.0;
-      for (int r = c + 1; r < jn; ++r) {
-        double s = 0.0;
-        for (int t = c; t < r; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
-        tri[r + c * 33] = -s;
-      }
-    }
-    __syncthreads();
-    const int below = b - jb - jn;
-    if (below > 0) {
-      // L[jb+jn:b, jb:jb+jn] is the strictly-lower part of Wm; X[jb+jn:, jb+jn:]
-      // (already final, zero above its diagonal) is in Li.
-      cta_gemm<double, GETRF_THREADS>(below, jn, below, 1.0, Li + (jb + jn) + (int64_t)(jb + jn) * ldA, ldA, false,
-                                      Wm + (jb + jn) + (int64_t)jb * b, b, false, 0.0, Gp, below, gsm);
-      cta_gemm<double, GETRF_THREADS>(below, jn, jn, -1.0, Gp, below, false, tri, 33, false, 0.0,
-                                      Li + (jb + jn) + (int64_t)jb * ldA, ldA, gsm);
-    }
-    for (int e = threadIdx.x; e < (jb + jn) * jn; e += blockDim.x) {
-      const int r = e % (jb + jn), c = e / (jb + jn);
-      Li[r + (int64_t)(jb + c) * ldA] = T((r >= jb) ? tri[(r - jb) + c * 33] : 0.0);
-    }
-    __syncthreads();
+  // upper: rows below the last diagonal row are zero; lower: rows above c0
+  const int rlo = upper ? 0 : c0, rhi = upper ? c0 + cn : b;
+  for (int e = threadIdx.x; e < b * cn; e += blockDim.x) {
+    const int r = e % b, c = e / b;
+    out[r + (int64_t)(c0 + c) * ld] = (r >= rlo && r < rhi) ? T(X[r + (int64_t)c * b]) : T(0);
   }
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    atomicAdd(ws.flops + FLOP_GETRF, (unsigned long long)(2.0 / 3.0 * (double)b * b * b));
 }
 
 // ---------------------------------------------------------------------------

@@ -26,7 +26,7 @@ enum ErrSlot {
 
 // Algorithmic FLOP counters (device unsigned long long array of the plan),
 // one per kernel class of the factorization.
-enum FlopSlot { FLOP_GETRF = 0, FLOP_PANEL = 1, FLOP_DENSE = 2, FLOP_RECOMP = 3, FLOP_SLOTS = 4 };
+enum FlopSlot { FLOP_GETRF = 0, FLOP_PANEL = 1, FLOP_DENSE = 2, FLOP_RECOMP = 3, FLOP_TRINV = 4, FLOP_SLOTS = 5 };
 
 FRANK_D double warp_sum(double v) {
 #pragma unroll
