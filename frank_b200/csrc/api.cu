@@ -146,6 +146,13 @@ bool use_gram(const frank_blr* p) {
   return p->precision == FRANK_PREC_MIXED && p->fixed_rank == 0 && p->core_method == CORE_RRQR && p->gram;
 }
 
+// Mixed plans with the RRQR core truncate the working copy to the factor
+// tolerance at reset (needs a recompression scratch slot of 4 k^2 + 8 k).
+bool pretruncate(const frank_blr* p) {
+  return p->precision == FRANK_PREC_MIXED && p->fixed_rank == 0 && p->core_method == CORE_RRQR && p->nlr > 0 &&
+         p->rstride >= 4 * (int64_t)p->kcap * p->kcap + 8 * (int64_t)p->kcap;
+}
+
 cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * FLOP_SLOTS + cls) * 2 + end]; }
 
 // Per-CTA scratch of the update / recompression kernels, sized by the grids.
@@ -172,6 +179,13 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   int64_t launches = 0;
   k_reset<T><<<p->nb * p->nb, 256, 0, s>>>(H, W);
   ++launches;
+  if (pretruncate(p)) {
+    // mixed plans: the factor's tolerance is looser than A_H's, so the working
+    // copy's low-rank blocks are truncated to it before the first step
+    k_truncate_lr<T><<<std::max(p->grid_recomp, p->grid_gram), TRUNC_THREADS, 0, s>>>(
+        H, W, ws, p->core_scale * p->eps, p->rscratch, p->rstride);
+    ++launches;
+  }
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
   CUDA_TRY(cudaMemsetAsync(p->work, 0, 2 * p->nb * sizeof(int), s));

@@ -141,15 +141,101 @@ __global__ void k_reset(BlrView<double> H, BlrView<T> W) {
 }
 
 // ---------------------------------------------------------------------------
+// K0': truncation of the working copy's low-rank blocks to the factor
+// tolerance (mixed plans, whose factor is computed at a looser tolerance
+// than A_H).  Block U S V^T of A_H with orthonormal U, V: truncated pivoted
+// QR of S to thr_scale * ||S||_F (the core truncation of the recompression,
+// geqp3.cpp:71-192), S P = Q R, then RQ of the kept rows R P^T = S' Q', so
+// W = (U Q_r) S' (V Q'^T)^T with rank r.  Blocks whose rank does not drop
+// keep the copy k_reset made.  One CTA per block (grid-stride), FP64
+// scratch slot per CTA (4 k^2 + 8 k doubles).
+// ---------------------------------------------------------------------------
+constexpr int TRUNC_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr(BlrView<double> H, BlrView<T> W, FactorWs<T> ws,
+                                                              double thr_scale, double* scratch, int64_t stride) {
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ double red[32];
+  __shared__ int redi[32];
+  double* base = scratch + (int64_t)blockIdx.x * stride;
+  const int nblk = H.nb * H.nb;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    if (H.lslot[blk] < 0) continue;
+    const int k = H.rank[blk];
+    if (k <= 1) continue;
+    const int i = blk / H.nb, j = blk % H.nb;
+    const int bi = H.bs(i), bj = H.bs(j);
+    double* M = base;                          // k x k
+    double* Xo = M + (int64_t)k * k;           // k x r
+    double* X2 = Xo + (int64_t)k * k;          // k x r
+    double* Qt = X2 + (int64_t)k * k;          // k x r
+    double* tau = Qt + (int64_t)k * k;
+    double* tau2 = tau + k;
+    double* cn = tau2 + k;
+    double* pn = cn + k;
+    int* jpvt = reinterpret_cast<int*>(pn + k);
+    int* jinv = jpvt + k;
+    const double* hs = H.s(i, j);
+    double f = 0.0;
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+      const double v = hs[(e % k) + (int64_t)(e / k) * H.kcap];
+      M[e] = v;
+      f += v * v;
+    }
+    f = block_sum(f, red);
+    const int r = cta_truncated_geqp3(k, k, M, k, thr_scale * sqrt(f), W.kcap, tau, cn, pn, jpvt, red, redi);
+    if (r >= k) continue;
+    T* wu = W.u(i, j); T* wsm = W.s(i, j); T* wv = W.vt(i, j);
+    if (r == 0) {
+      for (int e = threadIdx.x; e < bi; e += blockDim.x) wu[e] = T(e == 0 ? 1.0 : 0.0);
+      for (int e = threadIdx.x; e < bj; e += blockDim.x) wv[e] = T(e == 0 ? 1.0 : 0.0);
+      if (threadIdx.x == 0) { wsm[0] = T(0); W.rank[blk] = 1; }
+      __syncthreads();
+      continue;
+    }
+    // Xo = Q[:, :r]
+    for (int e = threadIdx.x; e < k * r; e += blockDim.x) Xo[e] = ((e % k) == (e / k)) ? 1.0 : 0.0;
+    for (int c = threadIdx.x; c < k; c += blockDim.x) jinv[jpvt[c]] = c;
+    __syncthreads();
+    cta_apply_q(k, r, M, k, tau, r, Xo, (int64_t)k);
+    // RQ of R P^T (r x k): QR of X2 = (R P^T)^T J
+    for (int e = threadIdx.x; e < k * r; e += blockDim.x) {
+      const int c = e % k, a = e / k;
+      const int row = r - 1 - a, src = jinv[c];
+      X2[e] = (row <= src) ? M[row + (int64_t)src * k] : 0.0;
+    }
+    __syncthreads();
+    cta_householder_qr(k, r, X2, k, tau2, red);
+    for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
+      const int a = e % r, c = e / r;
+      const int ra = r - 1 - c, ca = r - 1 - a;
+      wsm[a + (int64_t)c * W.kcap] = T((ra <= ca) ? X2[ra + (int64_t)ca * k] : 0.0);
+    }
+    for (int e = threadIdx.x; e < k * r; e += blockDim.x) Qt[e] = ((e % k) == (e / k)) ? 1.0 : 0.0;
+    __syncthreads();
+    cta_apply_q(k, r, X2, k, tau2, r, Qt, (int64_t)k);
+    // new U = U Xo; then Xo := Qt with its columns reversed, new V = V Xo
+    cta_gemm<double, TRUNC_THREADS>(bi, r, k, 1.0, H.u(i, j), H.bmax, false, Xo, k, false, 0.0, wu, W.bmax, gsm);
+    for (int e = threadIdx.x; e < k * r; e += blockDim.x) {
+      const int rr = e % k, a = e / k;
+      Xo[e] = Qt[rr + (int64_t)(r - 1 - a) * k];
+    }
+    __syncthreads();
+    cta_gemm<double, TRUNC_THREADS>(bj, r, k, 1.0, H.vt(i, j), H.bmax, false, Xo, k, false, 0.0, wv, W.bmax, gsm);
+    if (threadIdx.x == 0) W.rank[blk] = r;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K1: leaf getrf of diagonal block i with partial pivoting, FP64, one CTA
 // (512 threads).  Blocked right-looking LU (panel width 32): the panel is
 // factored column by column (idamax pivot, row swap across the whole block,
 // reciprocal scaling and rank-1 update as in LAPACK dgetf2), then the row
 // block is solved with the unit-lower 32x32 triangle and the trailing matrix
-// updated by a CTA GEMM.  Then the explicit inverses of the unit-lower L and
-// the upper U are formed by blocked triangular inversion (LAPACK dtrtri
-// column-block order).  Writes the packed LU back into the block, the
-// pivots/permutation, Linv and Uinv in T.
+// updated by a CTA GEMM.  Writes the packed LU back into the block and the
+// pivots/permutation; the explicit inverses Linv, Uinv are formed by k_trinv.
 // ---------------------------------------------------------------------------
 constexpr int GETRF_THREADS = 512;
 

@@ -326,21 +326,23 @@ FRANK_D void cta_larft(int mr, int jn, const double* smV, const double* tau, dou
     if (lane == 0) smT[i + j * QRB] = s;  // G(i,j), i<j, temporarily in T's upper part
   }
   __syncthreads();
-  // T column by column (dlarft recurrence), one warp: lane i owns row i.
+  // T column by column (dlarft recurrence), one warp: lane i < QRB owns row i.
   // G(l, j) (l < j) sits in T's upper part until column j is produced.
   if (threadIdx.x < 32) {
     const int i = threadIdx.x;
+    const bool row = i < QRB;
     for (int j = 0; j < jn; ++j) {
       double s = 0.0;
-      if (i < j)
+      if (row && i < j)
         for (int l = i; l < j; ++l) s += smT[i + l * QRB] * smT[l + j * QRB];
       __syncwarp();
-      if (i < j) smT[i + j * QRB] = -tau[j] * s;
+      if (row && i < j) smT[i + j * QRB] = -tau[j] * s;
       if (i == j) smT[j + j * QRB] = tau[j];
-      if (i > j) smT[i + j * QRB] = 0.0;
+      if (row && i > j) smT[i + j * QRB] = 0.0;
       __syncwarp();
     }
-    for (int j = jn; j < QRB; ++j) smT[i + j * QRB] = 0.0;
+    if (row)
+      for (int j = jn; j < QRB; ++j) smT[i + j * QRB] = 0.0;
   }
   __syncthreads();
 }
