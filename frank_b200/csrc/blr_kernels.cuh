@@ -630,7 +630,9 @@ FRANK_D UpdOps<T> update_operands(const BlrView<T>& A, const FactorWs<T>& ws, in
 template <typename T, int NT>
 FRANK_D void form_core(const UpdOps<T>& o, int bi, int ld, double* Tm, double* gsm) {
   if (!o.left_dense && !o.right_dense) {
-    cta_gemm<double, NT>(o.p, o.q, bi, -1.0, o.WL, ld, true, o.WU, ld, false, 0.0, Tm, o.p, gsm);
+    // small cores: one warp per entry (lanes along the b-long inner dimension)
+    if (o.p * o.q <= 1024) cta_gemm_tn_dot(o.p, o.q, bi, -1.0, o.WL, ld, o.WU, ld, Tm, o.p);
+    else cta_gemm<double, NT>(o.p, o.q, bi, -1.0, o.WL, ld, true, o.WU, ld, false, 0.0, Tm, o.p, gsm);
   } else if (!o.left_dense && o.right_dense) {
     // -WL^T (p x bi)
     for (int64_t e = threadIdx.x; e < (int64_t)o.p * o.q; e += blockDim.x) {
@@ -982,8 +984,9 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     if (threadIdx.x == 0)
       atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r));
     // U = Qu Xo ; Vt = Qv Yo  (blocked WY application)
-    cta_apply_q_blocked<RECOMP_THREADS>(bc, mu, Ash, bc, Tfu, r, Xo, (int64_t)bc, Wq, smP, smT, gsm);
-    cta_apply_q_blocked<RECOMP_THREADS>(bk, mv, Bsh, bk, Tfv, r, Yo, (int64_t)bk, Wq, smP, smT, gsm);
+    // Xo = [Q_core; 0], Yo = [V_core; 0]: rows at or below mu (mv) are zero
+    cta_apply_q_blocked<RECOMP_THREADS>(bc, mu, Ash, bc, Tfu, r, Xo, (int64_t)bc, Wq, smP, smT, gsm, mu);
+    cta_apply_q_blocked<RECOMP_THREADS>(bk, mv, Bsh, bk, Tfv, r, Yo, (int64_t)bk, Wq, smP, smT, gsm, mv);
     for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
       const int rr = e % bc, c = e / bc;
       Uc[rr + (int64_t)c * ld] = T(Xo[e]);

@@ -404,21 +404,28 @@ FRANK_D void cta_qr_blocked(int m, int n, double* A, int64_t lda, double* tau, d
 }
 
 // X (m x r, ldx, FP64) := Q X with Q from cta_qr_blocked (k = min(m, ncols)
-// reflectors).  Panels applied last to first: X -= V (T (V^T X)).
+// reflectors).  Panels applied last to first: X -= V (T (V^T X)).  Rows of X
+// at or below nz are zero on entry (nz = m if unknown): the first panel
+// applied then only contracts rows j0 .. nz-1 in V^T X.
 template <int NT>
 FRANK_D void cta_apply_q_blocked(int m, int k, const double* A, int64_t lda, const double* Tf, int r,
-                                 double* X, int64_t ldx, double* W, double* smP, double* smT, double* gsm) {
+                                 double* X, int64_t ldx, double* W, double* smP, double* smT, double* gsm,
+                                 int nz = -1) {
   if (k <= 0 || r <= 0) { __syncthreads(); return; }
+  if (nz < 0 || nz > m) nz = m;
   const int np = (k + QRB - 1) / QRB;
   for (int p = np - 1; p >= 0; --p) {
     const int j0 = p * QRB;
     const int jn = min(QRB, k - j0);
     const int mr = m - j0;
+    const int kr = min(mr, max(0, nz - j0));   // rows of X that can be nonzero
+    nz = m;                                    // after this panel X is full
+    if (kr == 0) continue;                     // V^T X = 0: the panel is the identity on X
     cta_load_v(mr, jn, A + j0 + (int64_t)j0 * lda, lda, smP);
     for (int e = threadIdx.x; e < QRB * QRB; e += blockDim.x) smT[e] = Tf[(int64_t)p * QRB * QRB + e];
     __syncthreads();
     double* Xp = X + j0;
-    cta_gemm<double, NT>(jn, r, mr, 1.0, smP, mr, true, Xp, ldx, false, 0.0, W, QRB, gsm);
+    cta_gemm<double, NT>(jn, r, kr, 1.0, smP, mr, true, Xp, ldx, false, 0.0, W, QRB, gsm);
     for (int c = threadIdx.x; c < r; c += blockDim.x) {
       double w[QRB];
       for (int i = 0; i < jn; ++i) w[i] = W[i + (int64_t)c * QRB];
