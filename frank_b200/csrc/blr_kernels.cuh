@@ -811,6 +811,11 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       if (threadIdx.x == 0) atomicAdd(ws.err + ERR_BOUNDS, 1);
       continue;
     }
+    const int cls = (su <= 64 && sv <= 64) ? 0 : 1;
+    PHASE_BEGIN();
+#ifdef FRANK_PHASE_TIMING
+    if (threadIdx.x == 0) atomicAdd(&g_phase_count[cls], 1ull);
+#endif
     T* Uc = A.u(ic, k);
     T* Sc = A.s(ic, k);
     T* Vc = A.vt(ic, k);
@@ -828,8 +833,11 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       Bsh[r + (int64_t)c * bk] = v;
     }
     form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
+    PHASE_MARK(cls, 0);
     cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
+    PHASE_MARK(cls, 1);
     cta_qr_blocked<RECOMP_THREADS>(bk, sv, Bsh, bk, tau_v, Tfv, Wq, smP, smT, gsm, red);
+    PHASE_MARK(cls, 2);
     const int mu = min(bc, su), mv = min(bk, sv);
     // clean upper-trapezoidal R factors
     for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
@@ -849,6 +857,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     const bool in_smem = (int64_t)mu * mv + 4 * (int64_t)mv + 2 * mu <= RECOMP_REGION;
     double* Mm = in_smem ? region : Mg;
     cta_gemm<double, RECOMP_THREADS>(mu, mv, sv, 1.0, Mtmp, mu, false, Rv, mv, true, 0.0, Mm, mu, gsm);
+    PHASE_MARK(cls, 3);
     int r = 0;
     if (core_method == CORE_RRQR && ws.fixed_rank == 0) {
       double f = 0.0;
@@ -872,17 +881,32 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
         atomicMax(ws.err + ERR_MAX_RANK, r);
         atomicAdd(ws.err + ERR_RECOMP, 1);
       }
+      // the small factors (Q_core, the RQ of its kept rows and its explicit Q)
+      // stay in shared memory after the core when they fit
+      const int64_t voff = (int64_t)mu * mv + 4 * (int64_t)mv + 2 * (int64_t)mu;
+      const bool t_sm = in_smem && voff + 2 * (int64_t)mv * r + (int64_t)mu * r <= RECOMP_REGION;
       // Xo (bc x r) = [Q_core; 0]
-      for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
-        const int rr = e % bc, c = e / bc;
-        Xo[e] = (rr == c) ? 1.0 : 0.0;
+      if (t_sm) {
+        double* X1s = region + voff + 2 * (int64_t)mv * r;   // mu x r
+        for (int64_t e = threadIdx.x; e < (int64_t)mu * r; e += blockDim.x) X1s[e] = ((e % mu) == (e / mu)) ? 1.0 : 0.0;
+        __syncthreads();
+        cta_apply_q(mu, r, Mm, mu, tc, r, X1s, (int64_t)mu);
+        for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+          const int rr = e % bc, c = e / bc;
+          Xo[e] = rr < mu ? X1s[rr + (int64_t)c * mu] : 0.0;
+        }
+      } else {
+        for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+          const int rr = e % bc, c = e / bc;
+          Xo[e] = (rr == c) ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        cta_apply_q(mu, r, Mm, mu, tc, r, Xo, (int64_t)bc);
       }
-      __syncthreads();
-      cta_apply_q(mu, r, Mm, mu, tc, r, Xo, (int64_t)bc);
       // X2 (mv x r) = R_perm^T J, R_perm[:, jpvt[c']] = R[:, c']
       for (int c = threadIdx.x; c < mv; c += blockDim.x) jinv[jpvt[c]] = c;
       __syncthreads();
-      double* X2 = Mtmp;
+      double* X2 = t_sm ? region + voff : Mtmp;
       for (int64_t e = threadIdx.x; e < (int64_t)mv * r; e += blockDim.x) {
         const int c = e % mv, a = e / mv;
         const int row = r - 1 - a, src = jinv[c];
@@ -896,8 +920,8 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
         const int ra = r - 1 - c, ca = r - 1 - a;
         Sc[a + (int64_t)c * A.kcap] = T((ra <= ca) ? X2[ra + (int64_t)ca * mv] : 0.0);
       }
-      // Qt (mv x r) explicit into Rc, then Yo[:, a] = [Qt[:, r-1-a]; 0]
-      double* Qt = Rc;
+      // Qt (mv x r) explicit, then Yo[:, a] = [Qt[:, r-1-a]; 0]
+      double* Qt = t_sm ? X2 + (int64_t)mv * r : Rc;
       for (int64_t e = threadIdx.x; e < (int64_t)mv * r; e += blockDim.x) {
         const int rr = e % mv, c = e / mv;
         Qt[e] = (rr == c) ? 1.0 : 0.0;
@@ -981,6 +1005,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       }
       __syncthreads();
     }
+    PHASE_MARK(cls, 4);
     if (threadIdx.x == 0)
       atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r));
     // U = Qu Xo ; Vt = Qv Yo  (blocked WY application)
@@ -997,6 +1022,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     }
     if (threadIdx.x == 0) A.rank[blk] = r;
     __syncthreads();
+    PHASE_MARK(cls, 5);
   }
 }
 
