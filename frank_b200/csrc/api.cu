@@ -1243,6 +1243,13 @@ extern "C" int frank_debug_getrf_cycles(unsigned long long* c8) {
   return FRANK_OK;
 }
 
+extern "C" int frank_debug_sub_cycles(unsigned long long* c16) {
+  CUDA_TRY(cudaMemcpyFromSymbol(c16, g_sub_cycles, sizeof(unsigned long long) * 16));
+  unsigned long long z[16] = {0};
+  CUDA_TRY(cudaMemcpyToSymbol(g_sub_cycles, z, sizeof(z)));
+  return FRANK_OK;
+}
+
 extern "C" int frank_debug_phase_cycles(unsigned long long* cycles16, unsigned long long* count2) {
   CUDA_TRY(cudaMemcpyFromSymbol(cycles16, g_phase_cycles, sizeof(unsigned long long) * 16));
   CUDA_TRY(cudaMemcpyFromSymbol(count2, g_phase_count, sizeof(unsigned long long) * 2));

@@ -819,6 +819,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     T* Uc = A.u(ic, k);
     T* Sc = A.s(ic, k);
     T* Vc = A.vt(ic, k);
+    SUB_BEGIN();
     // stacked bases in FP64
     for (int64_t e = threadIdx.x; e < (int64_t)bc * su; e += blockDim.x) {
       const int r = e % bc, c = e / bc;
@@ -832,7 +833,9 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       else v = double(o.YR[(c - kc) + (int64_t)r * ld]);  // A(i,k)^T
       Bsh[r + (int64_t)c * bk] = v;
     }
+    SUB_MARK(9);
     form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
+    SUB_MARK(10);
     PHASE_MARK(cls, 0);
     cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
     PHASE_MARK(cls, 1);

@@ -313,36 +313,136 @@ namespace frank {
 // ---------------------------------------------------------------------------
 constexpr int QRB = 32;
 
-// Gram-based T factor of the panel V (mr x jn, unit lower trapezoid in smV).
-FRANK_D void cta_larft(int mr, int jn, const double* smV, const double* tau, double* smT) {
-  // G = V^T V (upper part), then T column by column (dlarft recurrence).
+// After the call, p[0] of lane l holds the sum over the warp of p[l] (the 32
+// sums of a warp's 32-vectors, one per lane, by recursive halving: 31
+// exchanges instead of 32 butterfly reductions).
+FRANK_D void warp_transpose_sum(double (&p)[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 16; k >= 1; k >>= 1) {
+    const bool up = (lane & k) != 0;
+#pragma unroll
+    for (int i = 0; i < k; ++i) {
+      const double send = up ? p[i] : p[i + k];
+      const double keep = up ? p[i + k] : p[i];
+      p[i] = keep + __shfl_xor_sync(0xffffffffu, send, k);
+    }
+  }
+}
+
+// W (jn x r, ld QRB) = V^T X over rows [0, kr): V (jn <= 32 columns, ldv) in
+// shared memory, X (ldx) anywhere.  One warp per column of X, lanes down the
+// rows with jn partial sums each, then warp_transpose_sum.  Ends with a
+// block barrier.
+template <typename TX>
+FRANK_D void panel_vtx(int kr, int jn, const double* smV, int64_t ldv, const TX* X, int64_t ldx, int r, double* W) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int e = wid; e < jn * jn; e += nw) {
-    const int i = e % jn, j = e / jn;
-    if (i >= j) continue;
-    double s = 0.0;
-    for (int r = lane; r < mr; r += 32) s += smV[r + (int64_t)i * mr] * smV[r + (int64_t)j * mr];
-    s = warp_sum(s);
-    if (lane == 0) smT[i + j * QRB] = s;  // G(i,j), i<j, temporarily in T's upper part
+  // (column of X, half of V's columns) per warp: 16 partial sums per lane
+  const int halves = jn > 16 ? 2 : 1;
+  for (int t = wid; t < r * halves; t += nw) {
+    const int c = t / halves, j0 = (t % halves) * 16;
+    const int jm = min(16, jn - j0);
+    const TX* xc = X + (int64_t)c * ldx;
+    const double* vb = smV + (int64_t)j0 * ldv;
+    double p[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) p[j] = 0.0;
+    int row = lane;
+    for (; row + 96 < kr; row += 128) {
+      const double x0 = double(xc[row]), x1 = double(xc[row + 32]), x2 = double(xc[row + 64]),
+                   x3 = double(xc[row + 96]);
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (j < jm) {
+          const double* v = vb + (int64_t)j * ldv + row;
+          p[j] += v[0] * x0 + v[32] * x1 + v[64] * x2 + v[96] * x3;
+        }
+    }
+    for (; row < kr; row += 32) {
+      const double xv = double(xc[row]);
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (j < jm) p[j] += vb[row + (int64_t)j * ldv] * xv;
+    }
+    // recursive halving over 16 values, then one butterfly level: lane l
+    // (l < 16) ends with the sum of p[l]
+#pragma unroll
+    for (int k = 8; k >= 1; k >>= 1) {
+      const bool up = (lane & k) != 0;
+#pragma unroll
+      for (int i = 0; i < k; ++i) {
+        const double send = up ? p[i] : p[i + k];
+        const double keep = up ? p[i + k] : p[i];
+        p[i] = keep + __shfl_xor_sync(0xffffffffu, send, k);
+      }
+    }
+    const double tot = p[0] + __shfl_xor_sync(0xffffffffu, p[0], 16);
+    if (lane < jm) W[j0 + lane + (int64_t)c * QRB] = tot;
   }
   __syncthreads();
-  // T column by column (dlarft recurrence), one warp: lane i < QRB owns row i.
-  // G(l, j) (l < j) sits in T's upper part until column j is produced.
+}
+
+// X (rows [0, mr), r columns, ldx) -= V W with V (mr x jn, ldv) in shared
+// memory and W (jn x r, ld QRB): one thread per row, the row of V in
+// registers.  Ends with a block barrier.
+FRANK_D void panel_x_minus_vw(int mr, int jn, const double* smV, int64_t ldv, const double* W, int r, double* X,
+                              int64_t ldx) {
+  for (int row = threadIdx.x; row < mr; row += blockDim.x) {
+    double v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = (j < jn) ? smV[row + (int64_t)j * ldv] : 0.0;
+    int c = 0;
+    for (; c + 1 < r; c += 2) {
+      const double* w0 = W + (int64_t)c * QRB;
+      const double* w1 = w0 + QRB;
+      double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < jn) { a0 += v[j] * w0[j]; a1 += v[j] * w1[j]; }
+      double* x0 = X + row + (int64_t)c * ldx;
+      double* x1 = x0 + ldx;
+      const double y0 = *x0, y1 = *x1;
+      *x0 = y0 - a0;
+      *x1 = y1 - a1;
+    }
+    if (c < r) {
+      const double* w0 = W + (int64_t)c * QRB;
+      double a0 = 0.0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < jn) a0 += v[j] * w0[j];
+      X[row + (int64_t)c * ldx] -= a0;
+    }
+  }
+  __syncthreads();
+}
+
+// Gram-based T factor of the panel V (mr x jn, unit lower trapezoid in smV).
+FRANK_D void cta_larft(int mr, int jn, const double* smV, const double* tau, double* smT) {
+  // G = V^T V (jn x jn, in smT), then T column by column (dlarft recurrence
+  // T(0:j, j) = -tau_j T(0:j, 0:j) G(0:j, j)): lane i keeps row i of T in
+  // registers, so the recurrence needs no barrier between columns.
+  panel_vtx(mr, jn, smV, mr, smV, mr, jn, smT);
   if (threadIdx.x < 32) {
     const int i = threadIdx.x;
-    const bool row = i < QRB;
-    for (int j = 0; j < jn; ++j) {
-      double s = 0.0;
-      if (row && i < j)
-        for (int l = i; l < j; ++l) s += smT[i + l * QRB] * smT[l + j * QRB];
-      __syncwarp();
-      if (row && i < j) smT[i + j * QRB] = -tau[j] * s;
-      if (i == j) smT[j + j * QRB] = tau[j];
-      if (row && i > j) smT[i + j * QRB] = 0.0;
-      __syncwarp();
+    double trow[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) trow[l] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (j < jn) {
+        double s = 0.0;
+#pragma unroll
+        for (int l = 0; l < 32; ++l)
+          if (l < j && l >= i) s += trow[l] * smT[l + j * QRB];
+        if (i < j) trow[j] = -tau[j] * s;
+        else if (i == j) trow[j] = tau[j];
+      }
     }
-    if (row)
-      for (int j = jn; j < QRB; ++j) smT[i + j * QRB] = 0.0;
+    __syncwarp();
+#pragma unroll
+    for (int l = 0; l < 32; ++l)
+      if (i < QRB && l < QRB) smT[i + l * QRB] = (i < jn && l < jn && l >= i) ? trow[l] : 0.0;
   }
   __syncthreads();
 }
@@ -357,10 +457,28 @@ FRANK_D void cta_load_v(int mr, int jn, const double* Ap, int64_t lda, double* s
   __syncthreads();
 }
 
+#ifdef FRANK_PHASE_TIMING
+__device__ unsigned long long g_sub_cycles[16];
+#define SUB_BEGIN() long long _sb_t0 = clock64()
+#define SUB_MARK(k)                                                                         \
+  do {                                                                                      \
+    __syncthreads();                                                                        \
+    if (threadIdx.x == 0) {                                                                 \
+      const long long _t = clock64();                                                      \
+      atomicAdd(&g_sub_cycles[(k)], (unsigned long long)(_t - _sb_t0));                     \
+      _sb_t0 = _t;                                                                          \
+    }                                                                                       \
+  } while (0)
+#else
+#define SUB_BEGIN() do {} while (0)
+#define SUB_MARK(k) do {} while (0)
+#endif
+
 template <int NT>
 FRANK_D void cta_qr_blocked(int m, int n, double* A, int64_t lda, double* tau, double* Tf, double* W,
                             double* smP, double* smT, double* gsm, double* red) {
   const int kmin = m < n ? m : n;
+  SUB_BEGIN();
   for (int j0 = 0; j0 < kmin; j0 += QRB) {
     const int jn = min(QRB, kmin - j0);
     const int mr = m - j0;
@@ -370,35 +488,46 @@ FRANK_D void cta_qr_blocked(int m, int n, double* A, int64_t lda, double* tau, d
       smP[e] = Ap[r + (int64_t)c * lda];
     }
     __syncthreads();
+    SUB_MARK(0);
     cta_householder_qr(mr, jn, smP, mr, tau + j0, red);
+    SUB_MARK(1);
     for (int e = threadIdx.x; e < mr * jn; e += blockDim.x) {
       const int r = e % mr, c = e / mr;
       Ap[r + (int64_t)c * lda] = smP[e];
       smP[e] = (r > c) ? smP[e] : (r == c ? 1.0 : 0.0);
     }
     __syncthreads();
+    SUB_MARK(2);
     cta_larft(mr, jn, smP, tau + j0, smT);
     double* Tp = Tf + (int64_t)(j0 / QRB) * QRB * QRB;
     for (int e = threadIdx.x; e < QRB * QRB; e += blockDim.x) Tp[e] = smT[e];
+    SUB_MARK(3);
     const int nc = n - j0 - jn;
     if (nc > 0) {
       double* At = A + j0 + (int64_t)(j0 + jn) * lda;
       // W = V^T At (jn x nc)
-      cta_gemm<double, NT>(jn, nc, mr, 1.0, smP, mr, true, At, lda, false, 0.0, W, QRB, gsm);
+      panel_vtx(mr, jn, smP, mr, At, lda, nc, W);
       // W = T^T W (T upper triangular): column per thread
       for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        // unrolled over the panel width so that w stays in registers
         double w[QRB];
-        for (int i = 0; i < jn; ++i) w[i] = W[i + (int64_t)c * QRB];
-        for (int i = jn - 1; i >= 0; --i) {
-          double s = 0.0;
-          for (int l = 0; l <= i; ++l) s += smT[l + i * QRB] * w[l];
-          W[i + (int64_t)c * QRB] = s;
+#pragma unroll
+        for (int i = 0; i < QRB; ++i) w[i] = (i < jn) ? W[i + (int64_t)c * QRB] : 0.0;
+#pragma unroll
+        for (int i = QRB - 1; i >= 0; --i) {
+          if (i < jn) {
+            double s = 0.0;
+#pragma unroll
+            for (int l = 0; l <= i; ++l) s += smT[l + i * QRB] * w[l];
+            W[i + (int64_t)c * QRB] = s;
+          }
         }
       }
       __syncthreads();
       // At -= V W
-      cta_gemm<double, NT>(mr, nc, jn, -1.0, smP, mr, false, W, QRB, false, 1.0, At, lda, gsm);
+      panel_x_minus_vw(mr, jn, smP, mr, W, nc, At, lda);
     }
+    SUB_MARK(4);
   }
   __syncthreads();
 }
@@ -421,22 +550,33 @@ FRANK_D void cta_apply_q_blocked(int m, int k, const double* A, int64_t lda, con
     const int kr = min(mr, max(0, nz - j0));   // rows of X that can be nonzero
     nz = m;                                    // after this panel X is full
     if (kr == 0) continue;                     // V^T X = 0: the panel is the identity on X
+    SUB_BEGIN();
     cta_load_v(mr, jn, A + j0 + (int64_t)j0 * lda, lda, smP);
     for (int e = threadIdx.x; e < QRB * QRB; e += blockDim.x) smT[e] = Tf[(int64_t)p * QRB * QRB + e];
     __syncthreads();
+    SUB_MARK(5);
     double* Xp = X + j0;
-    cta_gemm<double, NT>(jn, r, kr, 1.0, smP, mr, true, Xp, ldx, false, 0.0, W, QRB, gsm);
+    panel_vtx(kr, jn, smP, mr, Xp, ldx, r, W);
+    SUB_MARK(6);
     for (int c = threadIdx.x; c < r; c += blockDim.x) {
+      // unrolled over the panel width so that w stays in registers
       double w[QRB];
-      for (int i = 0; i < jn; ++i) w[i] = W[i + (int64_t)c * QRB];
-      for (int i = 0; i < jn; ++i) {
-        double s = 0.0;
-        for (int l = i; l < jn; ++l) s += smT[i + l * QRB] * w[l];
-        W[i + (int64_t)c * QRB] = s;
+#pragma unroll
+      for (int i = 0; i < QRB; ++i) w[i] = (i < jn) ? W[i + (int64_t)c * QRB] : 0.0;
+#pragma unroll
+      for (int i = 0; i < QRB; ++i) {
+        if (i < jn) {
+          double s = 0.0;
+#pragma unroll
+          for (int l = i; l < QRB; ++l) s += smT[i + l * QRB] * w[l];
+          W[i + (int64_t)c * QRB] = s;
+        }
       }
     }
     __syncthreads();
-    cta_gemm<double, NT>(mr, r, jn, -1.0, smP, mr, false, W, QRB, false, 1.0, Xp, ldx, gsm);
+    SUB_MARK(7);
+    panel_x_minus_vw(mr, jn, smP, mr, W, r, Xp, ldx);
+    SUB_MARK(8);
   }
 }
 
