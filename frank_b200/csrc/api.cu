@@ -220,7 +220,10 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
     ++launches;
     const int mm = m * m;
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s, cudaEventRecordExternal));
-    k_update_dense<T><<<std::min(mm, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
+    {
+      const int nt = (p->bmax + DUPD_TILE - 1) / DUPD_TILE;
+      k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nt * nt, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
+    }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
     ++launches;
     CUDA_TRY(cudaEventRecord(p->dense_done[i], s));

@@ -661,6 +661,7 @@ FRANK_D void form_core(const UpdOps<T>& o, int bi, int ld, double* Tm, double* g
 // Persistent grid over the m*m targets of the step, skipping low-rank ones.
 // ---------------------------------------------------------------------------
 constexpr int DUPD_THREADS = 256;
+constexpr int DUPD_TILE = 64;     // output tile of a dense update task
 
 template <typename T>
 __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i) {
@@ -671,28 +672,38 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
   const int bi = A.bs(i);
   double* Tm = ws.dscratch + (int64_t)blockIdx.x * ws.dscratch_stride;
   T* X = reinterpret_cast<T*>(Tm + (int64_t)ld * ld);
-  for (int tsk = blockIdx.x; tsk < m * m; tsk += gridDim.x) {
-    const int ic = i + 1 + tsk / m, k = i + 1 + tsk % m;
+  // tasks: (target, 64 x 64 tile of C); the small core T is recomputed per
+  // tile, so the tiles of one target run on different CTAs
+  const int nt = (ld + DUPD_TILE - 1) / DUPD_TILE, tpb = nt * nt;
+  const int ldx = min(DUPD_TILE, ld);   // X (rn x q) fits the slot's ld x ld region
+  for (int tsk = blockIdx.x; tsk < m * m * tpb; tsk += gridDim.x) {
+    const int pair = tsk / tpb, tile = tsk % tpb;
+    const int ic = i + 1 + pair / m, k = i + 1 + pair % m;
     if (A.is_lr(ic, k)) continue;
     const int bc = A.bs(ic), bk = A.bs(k);
-    T* C = A.dense(ic, k);
+    const int r0 = (tile / nt) * DUPD_TILE, c0 = (tile % nt) * DUPD_TILE;
+    if (r0 >= bc || c0 >= bk) continue;
+    const int rn = min(DUPD_TILE, bc - r0), cn = min(DUPD_TILE, bk - c0);
+    T* C = A.dense(ic, k) + r0 + (int64_t)c0 * ld;
     UpdOps<T> o = update_operands(A, ws, i, ic, k);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0 && tile == 0)
       atomicAdd(ws.flops + FLOP_DENSE, (unsigned long long)(2.0 * bc * bk * o.q + 2.0 * bc * o.p * o.q +
                                                             2.0 * bi * o.p * o.q));
     if (o.left_dense && o.right_dense) {
       // C -= A(ic,i) A(i,k)
-      cta_gemm<T, DUPD_THREADS>(bc, bk, bi, T(-1), o.XL, ld, false, o.YR, ld, false, T(1), C, ld, gsmt);
+      cta_gemm<T, DUPD_THREADS>(rn, cn, bi, T(-1), o.XL + r0, ld, false, o.YR + (int64_t)c0 * ld, ld, false, T(1), C,
+                                ld, gsmt);
       continue;
     }
     form_core<T, DUPD_THREADS>(o, bi, ld, Tm, gsm);
-    // X = XL * T  (bc x q), accumulate in the working precision
-    cta_gemm<T, DUPD_THREADS>(bc, o.q, o.p, T(1), o.XL, ld, false, Tm, o.p, false, T(0), X, ld, gsmt);
-    // C += X * YR^T
+    // X = XL(r0 : r0+rn, :) T  (rn x q), accumulate in the working precision
+    cta_gemm<T, DUPD_THREADS>(rn, o.q, o.p, T(1), o.XL + r0, ld, false, Tm, o.p, false, T(0), X, ldx, gsmt);
+    // C(tile) += X * YR(c0 : c0+cn, :)^T
     if (!o.right_dense)
-      cta_gemm<T, DUPD_THREADS>(bc, bk, o.q, T(1), X, ld, false, o.YR, ld, true, T(1), C, ld, gsmt);
+      cta_gemm<T, DUPD_THREADS>(rn, cn, o.q, T(1), X, ldx, false, o.YR + c0, ld, true, T(1), C, ld, gsmt);
     else
-      cta_gemm<T, DUPD_THREADS>(bc, bk, o.q, T(1), X, ld, false, o.YR, ld, false, T(1), C, ld, gsmt);
+      cta_gemm<T, DUPD_THREADS>(rn, cn, o.q, T(1), X, ldx, false, o.YR + (int64_t)c0 * ld, ld, false, T(1), C,
+                                ld, gsmt);
   }
 }
 
