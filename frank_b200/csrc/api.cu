@@ -215,7 +215,13 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
     const int m = p->nb - i - 1;
     if (m == 0) break;
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
-    k_panel<T><<<2 * m, PANEL_THREADS, 0, s>>>(W, ws, i);
+    {
+      const int rt = (p->bmax + PANEL_TILE - 1) / PANEL_TILE;
+      k_panel_gather<T><<<dim3(m, rt), PANEL_THREADS, 0, s>>>(W, ws, i);
+      k_panel_mul<T><<<dim3(2 * m, rt), PANEL_THREADS, 0, s>>>(W, ws, i);
+      k_panel_fin<T><<<dim3(2 * m, rt), PANEL_THREADS, 0, s>>>(W, ws, i);
+      launches += 2;
+    }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 1), s, cudaEventRecordExternal));
     ++launches;
     const int mm = m * m;

@@ -506,79 +506,130 @@ __global__ void __launch_bounds__(TRINV_THREADS) k_trinv(BlrView<T> A, FactorWs<
 }
 
 // ---------------------------------------------------------------------------
-// K2: panel of step i.  Task t < m: column-panel block (i+1+t, i):
+// K2: panel of step i (trsm.cpp:92-115 with the leaf inverse; the pivots of
+// K1 applied).  Task t < m: column-panel block (i+1+t, i):
 //   low rank: V <- V Uinv (Vt <- Uinv^T Vt), then WL = Vt S^T;
 //   dense:    A <- A Uinv.
 // Task t >= m: row-panel block (i, i+1+t-m):
 //   low rank: U <- Linv P U, then WU = U S;   dense: A <- Linv P A.
-// (trsm.cpp:92-115 with the leaf inverse; the pivots of K1 applied.)
+// Three launches, each over (task, 64-row tile of the result), so that every
+// block is spread over several CTAs and no tile reads rows another tile of
+// the same launch writes:
+//   k_panel_gather  row tasks:    tmp = P U  (P A)                 -> WU[k]
+//   k_panel_mul     column tasks: tmp = Uinv^T Vt  (A Uinv)        -> WL[ic]
+//                   row tasks:    U = Linv tmp  (A = Linv tmp)
+//   k_panel_fin     column tasks: Vt = tmp, then WL = Vt S^T  (A = tmp)
+//                   row tasks:    WU = U S
 // ---------------------------------------------------------------------------
 constexpr int PANEL_THREADS = 256;
+constexpr int PANEL_TILE = 64;
 
 template <typename T>
-__global__ void __launch_bounds__(PANEL_THREADS) k_panel(BlrView<T> A, FactorWs<T> ws, int i) {
-  __shared__ T gsm[2 * 16 * 64];
+struct PanelTask {
+  bool col;      // column-panel block (else row-panel block)
+  bool lr;
+  int blk, rows, cols, r;   // result rows x cols (cols = rank for low rank)
+  T* tmp;
+};
+
+template <typename T>
+FRANK_D PanelTask<T> panel_task(const BlrView<T>& A, const FactorWs<T>& ws, int i, int t) {
   const int m = A.nb - i - 1;
-  const int t = blockIdx.x;
-  const int bi = A.bs(i);
-  const int ld = A.bmax;
-  const T* Li = ws.Linv + (int64_t)i * ld * ld;
-  const T* Ui = ws.Uinv + (int64_t)i * ld * ld;
-  const int* perm = ws.perm + (int64_t)i * ld;
-  if (threadIdx.x == 0) {
-    const int blk = (t < m) ? (i + 1 + t) * A.nb + i : i * A.nb + (i + 1 + (t - m));
-    const double kk = A.lslot[blk] >= 0 ? A.rank[blk] : A.bs(t < m ? i + 1 + t : i + 1 + (t - m));
-    atomicAdd(ws.flops + FLOP_PANEL, (unsigned long long)((double)bi * bi * kk));
-  }
-  if (t < m) {
+  const int bi = A.bs(i), ld = A.bmax;
+  PanelTask<T> P;
+  P.col = t < m;
+  if (P.col) {
     const int ic = i + 1 + t;
-    T* tmp = ws.WL + (int64_t)ic * ld * ld;
-    if (A.is_lr(ic, i)) {
-      const int r = A.rank[ic * A.nb + i];
-      T* vt = A.vt(ic, i);
-      // tmp = Uinv^T * Vt   (bi x r)
-      cta_gemm<T, PANEL_THREADS>(bi, r, bi, T(1), Ui, ld, true, vt, ld, false, T(0), tmp, ld, gsm);
-      for (int64_t e = threadIdx.x; e < (int64_t)bi * r; e += blockDim.x) {
-        const int rr = e % bi, c = e / bi;
-        vt[rr + (int64_t)c * ld] = tmp[rr + (int64_t)c * ld];
-      }
-      __syncthreads();
-      // WL = Vt * S^T
-      cta_gemm<T, PANEL_THREADS>(bi, r, r, T(1), vt, ld, false, A.s(ic, i), A.kcap, true, T(0), tmp, ld, gsm);
-    } else {
-      const int bc = A.bs(ic);
-      T* a = A.dense(ic, i);
-      // tmp = A * Uinv  (bc x bi), then copy back
-      cta_gemm<T, PANEL_THREADS>(bc, bi, bi, T(1), a, ld, false, Ui, ld, false, T(0), tmp, ld, gsm);
-      for (int64_t e = threadIdx.x; e < (int64_t)bc * bi; e += blockDim.x) {
-        const int rr = e % bc, c = e / bc;
-        a[rr + (int64_t)c * ld] = tmp[rr + (int64_t)c * ld];
-      }
-    }
+    P.blk = ic * A.nb + i;
+    P.tmp = ws.WL + (int64_t)ic * ld * ld;
+    P.lr = A.lslot[P.blk] >= 0;
+    P.r = P.lr ? A.rank[P.blk] : 0;
+    P.rows = P.lr ? bi : A.bs(ic);
+    P.cols = P.lr ? P.r : bi;
   } else {
     const int k = i + 1 + (t - m);
-    T* tmp = ws.WU + (int64_t)k * ld * ld;
-    if (A.is_lr(i, k)) {
-      const int r = A.rank[i * A.nb + k];
-      T* u = A.u(i, k);
-      for (int64_t e = threadIdx.x; e < (int64_t)bi * r; e += blockDim.x) {
-        const int rr = e % bi, c = e / bi;
-        tmp[rr + (int64_t)c * ld] = u[perm[rr] + (int64_t)c * ld];
-      }
-      __syncthreads();
-      cta_gemm<T, PANEL_THREADS>(bi, r, bi, T(1), Li, ld, false, tmp, ld, false, T(0), u, ld, gsm);
-      // WU = U * S
-      cta_gemm<T, PANEL_THREADS>(bi, r, r, T(1), u, ld, false, A.s(i, k), A.kcap, false, T(0), tmp, ld, gsm);
-    } else {
-      const int bk = A.bs(k);
-      T* a = A.dense(i, k);
-      for (int64_t e = threadIdx.x; e < (int64_t)bi * bk; e += blockDim.x) {
-        const int rr = e % bi, c = e / bi;
-        tmp[rr + (int64_t)c * ld] = a[perm[rr] + (int64_t)c * ld];
-      }
-      __syncthreads();
-      cta_gemm<T, PANEL_THREADS>(bi, bk, bi, T(1), Li, ld, false, tmp, ld, false, T(0), a, ld, gsm);
+    P.blk = i * A.nb + k;
+    P.tmp = ws.WU + (int64_t)k * ld * ld;
+    P.lr = A.lslot[P.blk] >= 0;
+    P.r = P.lr ? A.rank[P.blk] : 0;
+    P.rows = bi;
+    P.cols = P.lr ? P.r : A.bs(k);
+  }
+  return P;
+}
+
+template <typename T>
+FRANK_D T* panel_data(const BlrView<T>& A, const PanelTask<T>& P) {
+  const int bi_ = P.blk / A.nb, bj_ = P.blk % A.nb;
+  if (!P.lr) return A.dense(bi_, bj_);
+  return P.col ? A.vt(bi_, bj_) : A.u(bi_, bj_);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_gather(BlrView<T> A, FactorWs<T> ws, int i) {
+  const int m = A.nb - i - 1;
+  const PanelTask<T> P = panel_task(A, ws, i, m + blockIdx.x);
+  const int r0 = blockIdx.y * PANEL_TILE;
+  if (r0 >= P.rows) return;
+  const int rn = min(PANEL_TILE, P.rows - r0), ld = A.bmax;
+  const int* perm = ws.perm + (int64_t)i * ld;
+  const T* src = panel_data(A, P);
+  for (int e = threadIdx.x; e < rn * P.cols; e += blockDim.x) {
+    const int rr = r0 + e % rn, c = e / rn;
+    P.tmp[rr + (int64_t)c * ld] = src[perm[rr] + (int64_t)c * ld];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_mul(BlrView<T> A, FactorWs<T> ws, int i) {
+  __shared__ T gsm[2 * 16 * 64];
+  const int t = blockIdx.x;
+  const PanelTask<T> P = panel_task(A, ws, i, t);
+  const int r0 = blockIdx.y * PANEL_TILE;
+  const int bi = A.bs(i), ld = A.bmax;
+  if (threadIdx.x == 0 && blockIdx.y == 0) {
+    const double kk = P.lr ? P.r : (P.col ? P.rows : P.cols);
+    atomicAdd(ws.flops + FLOP_PANEL, (unsigned long long)((double)bi * bi * kk));
+  }
+  if (r0 >= P.rows) return;
+  const int rn = min(PANEL_TILE, P.rows - r0);
+  T* d = panel_data(A, P);
+  const T* Li = ws.Linv + (int64_t)i * ld * ld;
+  const T* Ui = ws.Uinv + (int64_t)i * ld * ld;
+  if (P.col) {
+    if (P.lr)   // tmp(rows) = Uinv^T(rows, :) Vt
+      cta_gemm<T, PANEL_THREADS>(rn, P.cols, bi, T(1), Ui + (int64_t)r0 * ld, ld, true, d, ld, false, T(0), P.tmp + r0,
+                                 ld, gsm);
+    else        // tmp(rows) = A(rows, :) Uinv
+      cta_gemm<T, PANEL_THREADS>(rn, P.cols, bi, T(1), d + r0, ld, false, Ui, ld, false, T(0), P.tmp + r0, ld, gsm);
+  } else {      // U(rows) = Linv(rows, :) P U   (A likewise)
+    cta_gemm<T, PANEL_THREADS>(rn, P.cols, bi, T(1), Li + r0, ld, false, P.tmp, ld, false, T(0), d + r0, ld, gsm);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_fin(BlrView<T> A, FactorWs<T> ws, int i) {
+  __shared__ T gsm[2 * 16 * 64];
+  const int t = blockIdx.x;
+  const PanelTask<T> P = panel_task(A, ws, i, t);
+  const int r0 = blockIdx.y * PANEL_TILE;
+  if (r0 >= P.rows) return;
+  if (!P.col && !P.lr) return;
+  const int rn = min(PANEL_TILE, P.rows - r0), ld = A.bmax;
+  T* d = panel_data(A, P);
+  const int bi_ = P.blk / A.nb, bj_ = P.blk % A.nb;
+  if (P.col) {
+    for (int e = threadIdx.x; e < rn * P.cols; e += blockDim.x) {
+      const int rr = r0 + e % rn, c = e / rn;
+      d[rr + (int64_t)c * ld] = P.tmp[rr + (int64_t)c * ld];
     }
+    __syncthreads();
+    if (P.lr)   // WL(rows) = Vt(rows) S^T
+      cta_gemm<T, PANEL_THREADS>(rn, P.r, P.r, T(1), d + r0, ld, false, A.s(bi_, bj_), A.kcap, true, T(0),
+                                 P.tmp + r0, ld, gsm);
+  } else {      // WU(rows) = U(rows) S
+    cta_gemm<T, PANEL_THREADS>(rn, P.r, P.r, T(1), d + r0, ld, false, A.s(bi_, bj_), A.kcap, false, T(0),
+                               P.tmp + r0, ld, gsm);
   }
 }
 
