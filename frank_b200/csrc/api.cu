@@ -193,7 +193,23 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   CUDA_TRY(cudaStreamWaitEvent(s2, p->fork, 0));
   auto getrf_on_aux = [&](int step) -> int {
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 0), s2, cudaEventRecordExternal));
-    k_getrf<T><<<1, GETRF_THREADS, 0, s2>>>(W, ws, step);
+    {
+      // leaf LU as load / (panel, tiled trailing update) x panels / store
+      const int b = p->off_h[step + 1] - p->off_h[step];
+      k_getrf_load<T><<<64, GETRF_AUX_THREADS, 0, s2>>>(W, ws, step);
+      for (int jb = 0; jb < b; jb += 32) {
+        k_getrf_panel<T><<<1, GETRF_THREADS, 0, s2>>>(W, ws, step, jb);
+        const int m2 = b - jb - std::min(32, b - jb);
+        if (m2 > 0) {
+          const int nt = (m2 + 63) / 64;
+          k_getrf_trail<T><<<nt * nt, GETRF_AUX_THREADS, 0, s2>>>(W, ws, step, jb);
+          ++launches;
+        }
+        ++launches;
+      }
+      k_getrf_store<T><<<64, GETRF_AUX_THREADS, 0, s2>>>(W, ws, step);
+      launches += 1;
+    }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 1), s2, cudaEventRecordExternal));
     CUDA_TRY(cudaEventRecord(p->getrf_done[step], s2));
     return FRANK_OK;

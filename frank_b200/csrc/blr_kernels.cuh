@@ -239,6 +239,142 @@ __global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr(BlrView<double> H
 // ---------------------------------------------------------------------------
 constexpr int GETRF_THREADS = 512;
 
+// One 32-column panel step of the leaf LU of a b x b FP64 matrix Wm (ld b):
+// partial-pivoted factorization of columns jb .. jb+jn-1 (in registers, one
+// row per thread, when b <= GETRF_THREADS; column steps on the global copy
+// otherwise), the panel's interchanges applied to every other column, and
+// U12 = L11^{-1} A12 (through the 32 x bmax scratch panel Gp).  Pivots into
+// piv[jb ..]; returns the first column with a zero pivot, or -1.  Called by
+// all threads of a GETRF_THREADS CTA.
+FRANK_D int getrf_panel_step(int b, int jb, double* Wm, double* Gp, int* piv, double* red, int* redi, double* gsm,
+                             double* tri, double* prow, double* xrow) {
+  const int jn = min(32, b - jb);
+  int zero = -1;
+  if (b <= GETRF_THREADS) {
+    // Panel in registers: thread t owns row t (t >= jb) and its jn panel
+    // entries; a column step is an arg-max, a row exchange through shared
+    // memory and a rank-1 update, with no global traffic.
+    const int t = threadIdx.x;
+    const bool own = (t >= jb && t < b);
+    double a[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) a[c] = (own && c < jn) ? Wm[t + (int64_t)(jb + c) * b] : 0.0;
+    for (int jj = 0; jj < jn; ++jj) {
+      const int j = jb + jj;
+      double v = -1.0;
+      int vi = -1;
+      if (t >= j && t < b) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) if (c == jj) v = fabs(a[c]);
+        vi = t;
+      }
+      double amax;
+      const int p = block_argmax_abs(v < 0.0 ? 0.0 : v, vi, red, redi, &amax);
+      if (threadIdx.x == 0) piv[j] = p;
+      if (amax == 0.0 && zero < 0) zero = j;
+      // the pivot row goes to row j, row j to row p
+      if (t == p) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) prow[c] = a[c];
+      }
+      if (t == j) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) xrow[c] = a[c];
+      }
+      __syncthreads();
+      if (t == j) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) a[c] = prow[c];
+      } else if (t == p) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) a[c] = xrow[c];
+      }
+      if (t > j && t < b && amax != 0.0) {
+        const double rcp = 1.0 / prow[jj];
+        double l = 0.0;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) if (c == jj) { a[c] *= rcp; l = a[c]; }
+#pragma unroll
+        for (int c = 0; c < 32; ++c) if (c > jj) a[c] -= l * prow[c];
+      }
+      __syncthreads();
+    }
+    if (own) {
+#pragma unroll
+      for (int c = 0; c < 32; ++c) if (c < jn) Wm[t + (int64_t)(jb + c) * b] = a[c];
+    }
+    __syncthreads();
+    // the panel's interchanges applied to the columns outside the panel
+    for (int c = threadIdx.x; c < b; c += blockDim.x) {
+      if (c >= jb && c < jb + jn) continue;
+      double* col = Wm + (int64_t)c * b;
+      for (int jj = 0; jj < jn; ++jj) {
+        const int j = jb + jj, p = piv[j];
+        if (p != j) { const double tmp = col[j]; col[j] = col[p]; col[p] = tmp; }
+      }
+    }
+    __syncthreads();
+  } else {
+    // blocks larger than the thread count: column steps on the global copy
+    for (int j = jb; j < jb + jn; ++j) {
+      double best = -1.0;
+      int bi = -1;
+      for (int r = j + threadIdx.x; r < b; r += blockDim.x) {
+        const double av = fabs(Wm[r + (int64_t)j * b]);
+        if (av > best) { best = av; bi = r; }
+      }
+      double amax;
+      const int p = block_argmax_abs(best < 0.0 ? 0.0 : best, bi, red, redi, &amax);
+      if (threadIdx.x == 0) piv[j] = p;
+      if (amax == 0.0 && zero < 0) zero = j;
+      if (p != j && amax != 0.0) {
+        for (int c = threadIdx.x; c < b; c += blockDim.x) {
+          const double tt = Wm[j + (int64_t)c * b];
+          Wm[j + (int64_t)c * b] = Wm[p + (int64_t)c * b];
+          Wm[p + (int64_t)c * b] = tt;
+        }
+      }
+      __syncthreads();
+      if (amax != 0.0) {
+        const double rcp = 1.0 / Wm[j + (int64_t)j * b];
+        for (int r = j + 1 + threadIdx.x; r < b; r += blockDim.x) Wm[r + (int64_t)j * b] *= rcp;
+      }
+      __syncthreads();
+      const int nr = b - j - 1, nc = jb + jn - j - 1;
+      for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
+        const int r = j + 1 + e % nr, c = j + 1 + e / nr;
+        Wm[r + (int64_t)c * b] -= Wm[r + (int64_t)j * b] * Wm[j + (int64_t)c * b];
+      }
+      __syncthreads();
+    }
+  }
+  // U12 = L11^{-1} A12: invert the unit-lower 32x32 L11 into tri, then a
+  // CTA GEMM into the scratch panel and back.
+  const int ncr = b - jb - jn;
+  if (ncr > 0) {
+    for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
+    __syncthreads();
+    if (threadIdx.x < jn) {
+      const int c = threadIdx.x;
+      tri[c + c * 33] = 1.0;
+      for (int r = c + 1; r < jn; ++r) {
+        double s = 0.0;
+        for (int t = c; t < r; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
+        tri[r + c * 33] = -s;
+      }
+    }
+    __syncthreads();
+    cta_gemm<double, GETRF_THREADS>(jn, ncr, jn, 1.0, tri, 33, false, Wm + jb + (int64_t)(jb + jn) * b, b, false,
+                                    0.0, Gp, 32, gsm);
+    for (int e = threadIdx.x; e < jn * ncr; e += blockDim.x) {
+      const int r = e % jn, c = e / jn;
+      Wm[(jb + r) + (int64_t)(jb + jn + c) * b] = Gp[r + (int64_t)c * 32];
+    }
+    __syncthreads();
+  }
+  return zero;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<T> ws, int i) {
   __shared__ double red[32];
@@ -266,130 +402,11 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
   __shared__ double xrow[32];          // row exchanged with the pivot row
   for (int jb = 0; jb < b; jb += 32) {
     const int jn = min(32, b - jb);
-    if (b <= GETRF_THREADS) {
-      // Panel in registers: thread t owns row t (t >= jb) and its jn panel
-      // entries; a column step is an arg-max, a row exchange through shared
-      // memory and a rank-1 update, with no global traffic.
-      const int t = threadIdx.x;
-      const bool own = (t >= jb && t < b);
-      double a[32];
-#pragma unroll
-      for (int c = 0; c < 32; ++c) a[c] = (own && c < jn) ? Wm[t + (int64_t)(jb + c) * b] : 0.0;
-      for (int jj = 0; jj < jn; ++jj) {
-        const int j = jb + jj;
-        double v = -1.0;
-        int vi = -1;
-        if (t >= j && t < b) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) if (c == jj) v = fabs(a[c]);
-          vi = t;
-        }
-        double amax;
-        const int p = block_argmax_abs(v < 0.0 ? 0.0 : v, vi, red, redi, &amax);
-        if (threadIdx.x == 0) piv[j] = p;
-        if (amax == 0.0 && first_zero < 0) first_zero = j;
-        // the pivot row goes to row j, row j to row p
-        if (t == p) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) prow[c] = a[c];
-        }
-        if (t == j) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) xrow[c] = a[c];
-        }
-        __syncthreads();
-        if (t == j) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) a[c] = prow[c];
-        } else if (t == p) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) a[c] = xrow[c];
-        }
-        if (t > j && t < b && amax != 0.0) {
-          const double rcp = 1.0 / prow[jj];
-          double l = 0.0;
-#pragma unroll
-          for (int c = 0; c < 32; ++c) if (c == jj) { a[c] *= rcp; l = a[c]; }
-#pragma unroll
-          for (int c = 0; c < 32; ++c) if (c > jj) a[c] -= l * prow[c];
-        }
-        __syncthreads();
-      }
-      if (own) {
-#pragma unroll
-        for (int c = 0; c < 32; ++c) if (c < jn) Wm[t + (int64_t)(jb + c) * b] = a[c];
-      }
-      __syncthreads();
-      // the panel's interchanges applied to the columns outside the panel
-      for (int c = threadIdx.x; c < b; c += blockDim.x) {
-        if (c >= jb && c < jb + jn) continue;
-        double* col = Wm + (int64_t)c * b;
-        for (int jj = 0; jj < jn; ++jj) {
-          const int j = jb + jj, p = piv[j];
-          if (p != j) { const double tmp = col[j]; col[j] = col[p]; col[p] = tmp; }
-        }
-      }
-      __syncthreads();
-    } else {
-      // blocks larger than the thread count: column steps on the global copy
-      for (int j = jb; j < jb + jn; ++j) {
-        double best = -1.0;
-        int bi = -1;
-        for (int r = j + threadIdx.x; r < b; r += blockDim.x) {
-          const double av = fabs(Wm[r + (int64_t)j * b]);
-          if (av > best) { best = av; bi = r; }
-        }
-        double amax;
-        const int p = block_argmax_abs(best < 0.0 ? 0.0 : best, bi, red, redi, &amax);
-        if (threadIdx.x == 0) piv[j] = p;
-        if (amax == 0.0 && first_zero < 0) first_zero = j;
-        if (p != j && amax != 0.0) {
-          for (int c = threadIdx.x; c < b; c += blockDim.x) {
-            const double tt = Wm[j + (int64_t)c * b];
-            Wm[j + (int64_t)c * b] = Wm[p + (int64_t)c * b];
-            Wm[p + (int64_t)c * b] = tt;
-          }
-        }
-        __syncthreads();
-        if (amax != 0.0) {
-          const double rcp = 1.0 / Wm[j + (int64_t)j * b];
-          for (int r = j + 1 + threadIdx.x; r < b; r += blockDim.x) Wm[r + (int64_t)j * b] *= rcp;
-        }
-        __syncthreads();
-        const int nr = b - j - 1, nc = jb + jn - j - 1;
-        for (int e = threadIdx.x; e < nr * nc; e += blockDim.x) {
-          const int r = j + 1 + e % nr, c = j + 1 + e / nr;
-          Wm[r + (int64_t)c * b] -= Wm[r + (int64_t)j * b] * Wm[j + (int64_t)c * b];
-        }
-        __syncthreads();
-      }
+    {
+      const int z = getrf_panel_step(b, jb, Wm, Gp, piv, red, redi, gsm, tri, prow, xrow);
+      if (z >= 0 && first_zero < 0) first_zero = z;
     }
     GPHASE(1);
-    // U12 = L11^{-1} A12: invert the unit-lower 32x32 L11 into tri, then a
-    // CTA GEMM into the scratch panel and back.
-    const int ncr = b - jb - jn;
-    if (ncr > 0) {
-      for (int e = threadIdx.x; e < 32 * 33; e += blockDim.x) tri[e] = 0.0;
-      __syncthreads();
-      if (threadIdx.x < jn) {
-        const int c = threadIdx.x;
-        tri[c + c * 33] = 1.0;
-        for (int r = c + 1; r < jn; ++r) {
-          double s = 0.0;
-          for (int t = c; t < r; ++t) s += Wm[(jb + r) + (int64_t)(jb + t) * b] * tri[t + c * 33];
-          tri[r + c * 33] = -s;
-        }
-      }
-      __syncthreads();
-      cta_gemm<double, GETRF_THREADS>(jn, ncr, jn, 1.0, tri, 33, false, Wm + jb + (int64_t)(jb + jn) * b, b, false,
-                                      0.0, Gp, 32, gsm);
-      for (int e = threadIdx.x; e < jn * ncr; e += blockDim.x) {
-        const int r = e % jn, c = e / jn;
-        Wm[(jb + r) + (int64_t)(jb + jn + c) * b] = Gp[r + (int64_t)c * 32];
-      }
-      __syncthreads();
-    }
-    GPHASE(2);
     const int m2 = b - jb - jn;
     if (m2 > 0)
       cta_gemm<double, GETRF_THREADS>(m2, m2, jn, -1.0, Wm + (jb + jn) + (int64_t)jb * b, b, false,
@@ -414,6 +431,86 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
   }
   __syncthreads();
   GPHASE(5);
+}
+
+// ---------------------------------------------------------------------------
+// K1 as separate launches (the factorization path): the same leaf LU, with
+// the trailing update of each 32-column panel spread over 64 x 64 tiles on
+// many CTAs instead of one.  Sequence for diagonal block i:
+//   k_getrf_load; for each panel: k_getrf_panel (one CTA: getrf_panel_step),
+//   k_getrf_trail (tiles); k_getrf_store.
+// Per element the same operations in the same order as k_getrf.
+// ---------------------------------------------------------------------------
+constexpr int GETRF_AUX_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_load(BlrView<T> A, FactorWs<T> ws, int i) {
+  const int b = A.bs(i), ld = A.bmax;
+  const T* Dp = A.dense(i, i);
+  double* Wm = ws.getrf_scratch;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)b * b;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = e % b, c = e / b;
+    Wm[r + (int64_t)c * b] = double(Dp[r + (int64_t)c * ld]);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_THREADS) k_getrf_panel(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
+  __shared__ double red[32];
+  __shared__ int redi[32];
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ double tri[32 * 33];
+  __shared__ double prow[32];
+  __shared__ double xrow[32];
+  const int b = A.bs(i);
+  if (jb >= b) return;
+  double* Wm = ws.getrf_scratch;
+  double* Gp = Wm + (int64_t)A.bmax * A.bmax;
+  int* piv = ws.ipiv + (int64_t)i * A.bmax;
+  const int z = getrf_panel_step(b, jb, Wm, Gp, piv, red, redi, gsm, tri, prow, xrow);
+  if (z >= 0 && threadIdx.x == 0) atomicCAS(ws.err + ERR_SINGULAR_STEP, 0, i + 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_trail(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
+  __shared__ double gsm[2 * 16 * 64];
+  const int b = A.bs(i);
+  if (jb >= b) return;
+  const int jn = min(32, b - jb), m2 = b - jb - jn;
+  if (m2 <= 0) return;
+  double* Wm = ws.getrf_scratch;
+  const int nt = (m2 + 63) / 64;
+  for (int tile = blockIdx.x; tile < nt * nt; tile += gridDim.x) {
+    const int r0 = (tile / nt) * 64, c0 = (tile % nt) * 64;
+    const int rn = min(64, m2 - r0), cn = min(64, m2 - c0);
+    cta_gemm<double, GETRF_AUX_THREADS>(rn, cn, jn, -1.0, Wm + (jb + jn + r0) + (int64_t)jb * b, b, false,
+                                        Wm + jb + (int64_t)(jb + jn + c0) * b, b, false, 1.0,
+                                        Wm + (jb + jn + r0) + (int64_t)(jb + jn + c0) * b, b, gsm);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_store(BlrView<T> A, FactorWs<T> ws, int i) {
+  const int b = A.bs(i), ld = A.bmax;
+  T* Dp = A.dense(i, i);
+  const double* Wm = ws.getrf_scratch;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(ws.flops + FLOP_GETRF, (unsigned long long)(2.0 / 3.0 * (double)b * b * b));
+    const int* piv = ws.ipiv + (int64_t)i * ld;
+    int* perm = ws.perm + (int64_t)i * ld;
+    // permutation from the interchanges: (P B)[r] = B[perm[r]]
+    for (int r = 0; r < b; ++r) perm[r] = r;
+    for (int r = 0; r < b; ++r) {
+      const int p = piv[r];
+      const int t = perm[r]; perm[r] = perm[p]; perm[p] = t;
+    }
+  }
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)b * b;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = e % b, c = e / b;
+    Dp[r + (int64_t)c * ld] = T(Wm[r + (int64_t)c * b]);
+  }
 }
 
 // ---------------------------------------------------------------------------
