@@ -178,13 +178,23 @@ FRANK_D void cta_gemm(int m, int n, int k, TACC alpha, const TA* __restrict__ A,
 // Warps take columns, lanes take rows.
 // ---------------------------------------------------------------------------
 FRANK_D void cta_householder_qr(int m, int n, double* A, int64_t lda, double* tau, double* red) {
+  // Two barriers per column: the warp that updates column j+1 also leaves
+  // that column's squared norm below its diagonal for step j+1 (red[30..31],
+  // double-buffered; block_sum uses red[0 .. nw-1], so blockDim.x <= 960).
   const int kmin = m < n ? m : n;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (kmin <= 0) return;
+  double* xn = red + 30;
+  {
+    double s = 0.0;
+    for (int r = 1 + threadIdx.x; r < m; r += blockDim.x) s += A[r] * A[r];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) xn[0] = s;
+    __syncthreads();
+  }
   for (int j = 0; j < kmin; ++j) {
     double* col = A + (int64_t)j * lda;
-    double s = 0.0;
-    for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) s += col[r] * col[r];
-    const double xnorm2 = block_sum(s, red);
+    const double xnorm2 = xn[j & 1];
     const double alpha = col[j];
     double t = 0.0, beta = alpha, scal = 0.0;
     if (xnorm2 > 0.0) {
@@ -192,23 +202,27 @@ FRANK_D void cta_householder_qr(int m, int n, double* A, int64_t lda, double* ta
       beta = alpha >= 0.0 ? -nrm : nrm;
       t = (beta - alpha) / beta;
       scal = 1.0 / (alpha - beta);
-    }
-    // scale v and set the diagonal
-    if (xnorm2 > 0.0)
       for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) col[r] *= scal;
+    }
     __syncthreads();
     if (threadIdx.x == 0) { col[j] = beta; tau[j] = t; }
-    __syncthreads();
-    if (t != 0.0) {
-      // apply H = I - t v v^T to columns j+1..n-1
-      for (int c = j + 1 + wid; c < n; c += nw) {
-        double* cc = A + (int64_t)c * lda;
+    // apply H = I - t v v^T to columns j+1..n-1 (v_j = 1 implicit; rows > j)
+    for (int c = j + 1 + wid; c < n; c += nw) {
+      double* cc = A + (int64_t)c * lda;
+      if (t != 0.0) {
         double w = 0.0;
         if (lane == 0) w = cc[j];
         for (int r = j + 1 + lane; r < m; r += 32) w += col[r] * cc[r];
         w = warp_sum(w) * t;
         if (lane == 0) cc[j] -= w;
         for (int r = j + 1 + lane; r < m; r += 32) cc[r] -= w * col[r];
+      }
+      if (c == j + 1) {
+        __syncwarp();
+        double s2 = 0.0;
+        for (int r = j + 2 + lane; r < m; r += 32) s2 += cc[r] * cc[r];
+        s2 = warp_sum(s2);
+        if (lane == 0) xn[(j + 1) & 1] = s2;
       }
     }
     __syncthreads();
