@@ -1275,6 +1275,15 @@ extern "C" int frank_debug_sub_cycles(unsigned long long* c16) {
   return FRANK_OK;
 }
 
+extern "C" int frank_debug_tlog(long long* out, unsigned long long* n) {
+  CUDA_TRY(cudaMemcpyFromSymbol(n, g_tlog_n, sizeof(unsigned long long)));
+  const unsigned long long k = *n < 200000 ? *n : 200000;
+  if (out) CUDA_TRY(cudaMemcpyFromSymbol(out, g_tlog, sizeof(long long) * 6 * k));
+  unsigned long long z = 0;
+  CUDA_TRY(cudaMemcpyToSymbol(g_tlog_n, &z, sizeof(z)));
+  return FRANK_OK;
+}
+
 extern "C" int frank_debug_phase_cycles(unsigned long long* cycles16, unsigned long long* count2) {
   CUDA_TRY(cudaMemcpyFromSymbol(cycles16, g_phase_cycles, sizeof(unsigned long long) * 16));
   CUDA_TRY(cudaMemcpyFromSymbol(count2, g_phase_count, sizeof(unsigned long long) * 2));

@@ -66,6 +66,11 @@ __device__ unsigned long long g_phase_count[2];
 #define PHASE_BEGIN() do {} while (0)
 #define PHASE_MARK(cls, k) do {} while (0)
 #endif
+#ifdef FRANK_PHASE_TIMING
+__device__ unsigned long long g_tlog_n;
+__device__ long long g_tlog[200000][6];
+FRANK_D long long gtimer() { long long t; asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t)); return t; }
+#endif
 
 // Per-factorization workspace (device pointers).
 template <typename T>
@@ -874,7 +879,7 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
 // The core lives in shared memory when it fits (RECOMP_SMEM_CORE doubles).
 // ---------------------------------------------------------------------------
 constexpr int RECOMP_THREADS = 512;
-constexpr int RECOMP_SMEM_BYTES = 200 * 1024;           // dynamic shared memory
+constexpr int RECOMP_SMEM_BYTES = 227 * 1024 - 512;     // dynamic shared memory (all but the static part)
 constexpr int RECOMP_GSM = 2 * 16 * 64;                 // cta_gemm tiles (doubles)
 constexpr int RECOMP_REGION = RECOMP_SMEM_BYTES / 8 - RECOMP_GSM;  // doubles for panels / core
 enum CoreMethod { CORE_RRQR = 0, CORE_SVD = 1 };
@@ -972,6 +977,9 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     }
     const int cls = (su <= 64 && sv <= 64) ? 0 : 1;
     PHASE_BEGIN();
+#ifdef FRANK_PHASE_TIMING
+    const long long t_start = gtimer();
+#endif
 #ifdef FRANK_PHASE_TIMING
     if (threadIdx.x == 0) atomicAdd(&g_phase_count[cls], 1ull);
 #endif
@@ -1185,6 +1193,15 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     if (threadIdx.x == 0) A.rank[blk] = r;
     __syncthreads();
     PHASE_MARK(cls, 5);
+#ifdef FRANK_PHASE_TIMING
+    if (threadIdx.x == 0) {
+      const unsigned long long q = atomicAdd(&g_tlog_n, 1ull);
+      if (q < 200000) {
+        g_tlog[q][0] = i; g_tlog[q][1] = su; g_tlog[q][2] = sv; g_tlog[q][3] = r;
+        g_tlog[q][4] = t_start; g_tlog[q][5] = gtimer();
+      }
+    }
+#endif
   }
 }
 
