@@ -200,6 +200,12 @@ class BLRMatrix:
               "frank_blr_refine_device")
         return it.value, res.value
 
+    def set_grid(self, ctas: int):
+        """Limit the update / recompression grids to `ctas` thread blocks
+        (plans that run concurrently in a batch); every target then runs on
+        one CTA."""
+        check(lib().frank_blr_set_grid(self._h, int(ctas)), "frank_blr_set_grid")
+
     def set_timing(self, on: bool = True):
         """Record per-class kernel times inside the factorization graph (off
         by default: the event nodes serialise the graph's concurrent branches)."""

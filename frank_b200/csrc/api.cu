@@ -60,6 +60,8 @@ struct frank_blr {
   int *perm = nullptr, *ipiv = nullptr, *err = nullptr, *work = nullptr;
   void *Linv = nullptr, *Uinv = nullptr, *WL = nullptr, *WU = nullptr;
   double *getrf_scratch = nullptr, *dscratch = nullptr, *rscratch = nullptr;
+  double* rsplit = nullptr;     // scratch slots of split recompression targets
+  int* split_done = nullptr;    // [nb][SPLIT_MAX] side counters
   int64_t dstride = 0, rstride = 0;
   int grid_dense = 0, grid_recomp = 0, smax = 0;
   int core_method = CORE_RRQR;
@@ -155,9 +157,17 @@ bool pretruncate(const frank_blr* p) {
 
 cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * FLOP_SLOTS + cls) * 2 + end]; }
 
+// Split recompression targets (two CTAs per large band-1 target) on plans
+// with the full recompression grid (not the reduced grids of batched plans).
+bool split_on(const frank_blr* p) { return p->nb > 2 && p->grid_recomp >= p->sm_count - 1; }
+
 // Per-CTA scratch of the update / recompression kernels, sized by the grids.
 int ensure_scratch(frank_blr* p) {
   if (!p->dscratch) CUDA_TRY(dalloc(&p->dscratch, (size_t)p->grid_dense * p->dstride));
+  if (p->nlr > 0 && split_on(p) && !p->rsplit) {
+    CUDA_TRY(dalloc(&p->rsplit, (size_t)SPLIT_MAX * p->rstride));
+    CUDA_TRY(dalloc(&p->split_done, (size_t)p->nb * SPLIT_MAX));
+  }
   if (p->nlr > 0 && !p->rscratch)
     CUDA_TRY(dalloc(&p->rscratch, (size_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
                                       p->rstride));
@@ -189,6 +199,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
   CUDA_TRY(cudaMemsetAsync(p->work, 0, 2 * p->nb * sizeof(int), s));
+  if (p->split_done) CUDA_TRY(cudaMemsetAsync(p->split_done, 0, (size_t)p->nb * SPLIT_MAX * sizeof(int), s));
   CUDA_TRY(cudaEventRecord(p->fork, s));
   CUDA_TRY(cudaStreamWaitEvent(s2, p->fork, 0));
   auto getrf_on_aux = [&](int step) -> int {
@@ -262,12 +273,13 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
         ++launches;
         if (p->dense_offdiag) {
           k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i);
+              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr);
           ++launches;
         }
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-            W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0, p->work + i);
+            W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0, p->work + i,
+            p->rsplit ? SPLIT_MAX : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr);
         ++launches;
       }
     }
@@ -470,7 +482,8 @@ void free_plan(frank_blr* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   void* ptrs[] = {p->d_off, p->d_dslot, p->d_lslot, p->d_rankH, p->d_rankW, p->Hd, p->Hu, p->Hs, p->Hv,
                   p->Wd, p->Wu, p->Ws, p->Wv, p->perm, p->ipiv, p->err, p->work, p->Linv, p->Uinv, p->WL, p->WU,
-                  p->getrf_scratch, p->dscratch, p->rscratch, p->z, p->stmp, p->sctmp, p->part, p->vtmp, p->nrm};
+                  p->getrf_scratch, p->dscratch, p->rscratch, p->z, p->stmp, p->sctmp, p->part, p->vtmp, p->nrm,
+                  p->rsplit, p->split_done};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->flops) cudaFree(p->flops);
   for (cudaEvent_t e : p->ev) if (e) cudaEventDestroy(e);
@@ -1119,6 +1132,8 @@ extern "C" int frank_blr_set_grid(frank_blr* p, int ctas) {
   p->grid_dense = std::max(1, std::min({nb * nb, 2 * p->sm_count, ctas}));
   if (p->rscratch) { cudaFree(p->rscratch); p->rscratch = nullptr; }
   if (p->dscratch) { cudaFree(p->dscratch); p->dscratch = nullptr; }
+  if (p->rsplit) { cudaFree(p->rsplit); p->rsplit = nullptr; }
+  if (p->split_done) { cudaFree(p->split_done); p->split_done = nullptr; }
   if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
   if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
   p->factored = false;

@@ -879,6 +879,8 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
 // The core lives in shared memory when it fits (RECOMP_SMEM_CORE doubles).
 // ---------------------------------------------------------------------------
 constexpr int RECOMP_THREADS = 512;
+constexpr int SPLIT_P = 48;       // split band-1 targets whose operand rank exceeds this
+constexpr int SPLIT_MAX = 32;     // band-1 tasks eligible for the split (scratch slots)
 constexpr int RECOMP_SMEM_BYTES = 227 * 1024 - 512;     // dynamic shared memory (all but the static part)
 constexpr int RECOMP_GSM = 2 * 16 * 64;                 // cta_gemm tiles (doubles)
 constexpr int RECOMP_REGION = RECOMP_SMEM_BYTES / 8 - RECOMP_GSM;  // doubles for panels / core
@@ -922,7 +924,8 @@ FRANK_HD RecompLayout recomp_layout(int bmax, int smax) {
 template <typename T>
 __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
                                                                int core_method, double core_scale,
-                                                               int only_dense_operands, int* counter) {
+                                                               int only_dense_operands, int* counter, int nsplit,
+                                                               double* split_base, int* split_done) {
   extern __shared__ double dsm[];
   double* gsm = dsm;
   double* region = dsm + RECOMP_GSM;
@@ -934,38 +937,42 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
   const int ld = A.bmax;
   const int bi = A.bs(i);
   const RecompLayout L = recomp_layout(A.bmax, smax);
-  double* base = ws.rscratch + (int64_t)blockIdx.x * ws.rscratch_stride;
-  double* Ash = base + L.ash;
-  double* Bsh = base + L.bsh;
-  double* Tm = base + L.tm;
-  double* Rc = base + L.rc;
-  double* Rv = base + L.rv;
-  double* Mtmp = base + L.mtmp;
-  double* Mg = base + L.mglob;
-  double* M0 = base + L.m0;
-  double* Xo = base + L.xo;
-  double* Yo = base + L.yo;
-  double* Tfu = base + L.tfu;
-  double* Tfv = base + L.tfv;
-  double* Wq = base + L.w;
-  double* tau_u = base + L.tau_u;
-  double* tau_v = base + L.tau_v;
-  double* tau_c = base + L.tau_c;
-  double* tau2 = base + L.tau2;
-  double* cnorm = base + L.cn;
-  double* pnorm = base + L.pn;
-  int* jpvt = reinterpret_cast<int*>(base + L.jp);
-  int* jinv = reinterpret_cast<int*>(base + L.ji);
+  double* const cta_base = ws.rscratch + (int64_t)blockIdx.x * ws.rscratch_stride;
+  double *Ash, *Bsh, *Tm, *Rc, *Rv, *Mtmp, *Mg, *M0, *Xo, *Yo, *Tfu, *Tfv, *Wq, *tau_u, *tau_v, *tau_c, *tau2, *cnorm,
+      *pnorm;
+  int *jpvt, *jinv;
+  auto set_base = [&](double* base) {
+    Ash = base + L.ash; Bsh = base + L.bsh; Tm = base + L.tm; Rc = base + L.rc; Rv = base + L.rv;
+    Mtmp = base + L.mtmp; Mg = base + L.mglob; M0 = base + L.m0; Xo = base + L.xo; Yo = base + L.yo;
+    Tfu = base + L.tfu; Tfv = base + L.tfv; Wq = base + L.w; tau_u = base + L.tau_u; tau_v = base + L.tau_v;
+    tau_c = base + L.tau_c; tau2 = base + L.tau2; cnorm = base + L.cn; pnorm = base + L.pn;
+    jpvt = reinterpret_cast<int*>(base + L.jp); jinv = reinterpret_cast<int*>(base + L.ji);
+  };
+  __shared__ int s_last;
   double* smP = region;
   double* smT = region + (int64_t)A.bmax * QRB;
   __shared__ int s_task;
   const int ntask = m * (m - 1);
-  for (int tsk = next_task(counter, &s_task); tsk < ntask; tsk = next_task(counter, &s_task)) {
+  // Split targets: band-1 targets (the first 2(m-1) tasks, largest ranks)
+  // whose operands have ranks above SPLIT_P get one task per side of the
+  // stacked-basis QR, run on two CTAs into the target's own scratch slot;
+  // the CTA that finishes second does the rest (no waiting).  The test uses
+  // only operand ranks, which no CTA changes during the launch.
+  const int nspl = split_base ? min(nsplit, 2 * (m - 1)) : 0;
+  const int ntot = 2 * nspl + ntask;
+  for (int q = next_task(counter, &s_task); q < ntot; q = next_task(counter, &s_task)) {
+    const int side = q < 2 * nspl ? (q & 1) : -1;
+    const int tsk = q < 2 * nspl ? (q >> 1) : q - 2 * nspl;
     int a_, c_;
     band_task(m, tsk, a_, c_);
     const int ic = i + 1 + a_, k = i + 1 + c_;
     if (!A.is_lr(ic, k)) continue;
     if (only_dense_operands && A.is_lr(ic, i) && A.is_lr(i, k)) continue;
+    const bool split_t = tsk < nspl && A.is_lr(ic, i) && A.is_lr(i, k) &&
+                         max(A.rank[ic * A.nb + i], A.rank[i * A.nb + k]) > SPLIT_P;
+    if ((side >= 0) != split_t) continue;
+    set_base(side >= 0 ? split_base + (int64_t)tsk * ws.rscratch_stride : cta_base);
+    const bool do_u = side != 1, do_v = side != 0;
     const int blk = ic * A.nb + k;
     const int bc = A.bs(ic), bk = A.bs(k);
     const int kc = A.rank[blk];
@@ -988,11 +995,11 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     T* Vc = A.vt(ic, k);
     SUB_BEGIN();
     // stacked bases in FP64
-    for (int64_t e = threadIdx.x; e < (int64_t)bc * su; e += blockDim.x) {
+    for (int64_t e = threadIdx.x; do_u && e < (int64_t)bc * su; e += blockDim.x) {
       const int r = e % bc, c = e / bc;
       Ash[r + (int64_t)c * bc] = (c < kc) ? double(Uc[r + (int64_t)c * ld]) : double(o.XL[r + (int64_t)(c - kc) * ld]);
     }
-    for (int64_t e = threadIdx.x; e < (int64_t)bk * sv; e += blockDim.x) {
+    for (int64_t e = threadIdx.x; do_v && e < (int64_t)bk * sv; e += blockDim.x) {
       const int r = e % bk, c = e / bk;
       double v;
       if (c < kc) v = double(Vc[r + (int64_t)c * ld]);
@@ -1001,13 +1008,24 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       Bsh[r + (int64_t)c * bk] = v;
     }
     SUB_MARK(9);
-    form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
+    if (do_u) form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
     SUB_MARK(10);
     PHASE_MARK(cls, 0);
-    cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
+    if (do_u) cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
     PHASE_MARK(cls, 1);
-    cta_qr_blocked<RECOMP_THREADS>(bk, sv, Bsh, bk, tau_v, Tfv, Wq, smP, smT, gsm, red);
+    // the V side of a split target works in Mtmp (free until the core), so
+    // that the two sides never share the W scratch
+    if (do_v) cta_qr_blocked<RECOMP_THREADS>(bk, sv, Bsh, bk, tau_v, Tfv, side == 1 ? Mtmp : Wq, smP, smT, gsm, red);
     PHASE_MARK(cls, 2);
+    if (side >= 0) {
+      // publish this side; the second of the two CTAs goes on with the target
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) s_last = atomicAdd(split_done + tsk, 1);
+      __syncthreads();
+      if (s_last == 0) continue;
+      __threadfence();
+    }
     const int mu = min(bc, su), mv = min(bk, sv);
     // clean upper-trapezoidal R factors
     for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {

@@ -187,3 +187,35 @@ def test_device_fixed_rank_construction_matches_oracle(gpu_lib):
     xg = M.solve(bv)
     xd = np.linalg.solve(fo.to_dense(A), bv)
     assert np.linalg.norm(xg - xd) <= FACTOR * np.linalg.norm(xo - xd) + 1e-13 * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_split_targets_match_one_cta(gpu_lib, precision):
+    """Large band-1 targets are recompressed by two CTAs (one per side of the
+    stacked-basis QR, the second to finish completes the target); a plan on a
+    reduced grid does every target on one CTA.  Same operations per target,
+    so the two factors are bitwise equal."""
+    from frank_b200 import BLRMatrix
+    n, nb = 8192, 16
+    rng = np.random.default_rng(31)
+    x, _ = fo.morton_sort(rng.random((3, n)), 12)
+    mats = []
+    for grid in (0, 64):
+        M = BLRMatrix(n, nb, eps=1e-8 if precision == "fp64" else 1e-3, precision=precision)
+        M.build_kernel("laplace", x, 1e-8)
+        if grid:
+            M.set_grid(grid)
+        M.getrf()
+        mats.append(M)
+    A, B = mats
+    assert max(A.rank(i + 1, i, 0) for i in range(nb - 1)) > 48   # the split path is exercised
+    assert A.stats()["recompressions"] == B.stats()["recompressions"] > 0
+    for i in range(nb):
+        for j in range(nb):
+            ba, bb = A.block(i, j, 1), B.block(i, j, 1)
+            if isinstance(ba, tuple):
+                assert A.rank(i, j, 1) == B.rank(i, j, 1), (i, j)
+                for u, v in zip(ba, bb):
+                    assert np.array_equal(u, v), (i, j)
+            else:
+                assert np.array_equal(ba, bb), (i, j)
