@@ -61,6 +61,8 @@ struct frank_blr {
   void *Linv = nullptr, *Uinv = nullptr, *WL = nullptr, *WU = nullptr;
   double *getrf_scratch = nullptr, *dscratch = nullptr, *rscratch = nullptr;
   double* rsplit = nullptr;     // scratch slots of split recompression targets
+  double* host_io = nullptr;    // device copies of b and x for frank_blr_refine
+  size_t host_io_cap = 0;
   int* split_done = nullptr;    // [nb][SPLIT_MAX] side counters
   int64_t dstride = 0, rstride = 0;
   int grid_dense = 0, grid_recomp = 0, smax = 0;
@@ -483,7 +485,7 @@ void free_plan(frank_blr* p) {
   void* ptrs[] = {p->d_off, p->d_dslot, p->d_lslot, p->d_rankH, p->d_rankW, p->Hd, p->Hu, p->Hs, p->Hv,
                   p->Wd, p->Wu, p->Ws, p->Wv, p->perm, p->ipiv, p->err, p->work, p->Linv, p->Uinv, p->WL, p->WU,
                   p->getrf_scratch, p->dscratch, p->rscratch, p->z, p->stmp, p->sctmp, p->part, p->vtmp, p->nrm,
-                  p->rsplit, p->split_done};
+                  p->rsplit, p->split_done, p->host_io};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (p->flops) cudaFree(p->flops);
   for (cudaEvent_t e : p->ev) if (e) cudaEventDestroy(e);
@@ -999,9 +1001,18 @@ int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int6
   if (!p || !b || !x || nrhs < 1 || ldb < p->n || ldx < p->n || maxit < 0)
     return fail(FRANK_ERR_INVALID, "bad refine arguments");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  double *db = nullptr, *dx = nullptr;
-  CUDA_TRY(cudaMalloc(&db, sizeof(double) * p->n * nrhs));
-  CUDA_TRY(cudaMalloc(&dx, sizeof(double) * p->n * nrhs));
+  // device copies of b and x: kept by the plan and grown on demand, so that
+  // repeated solves do not allocate
+  const size_t need = (size_t)p->n * nrhs;
+  if (need > p->host_io_cap) {
+    if (p->host_io) cudaFree(p->host_io);
+    p->host_io = nullptr;
+    p->host_io_cap = 0;
+    CUDA_TRY(cudaMalloc(&p->host_io, 2 * need * sizeof(double)));
+    p->host_io_cap = need;
+  }
+  double* db = p->host_io;
+  double* dx = p->host_io + need;
   CUDA_TRY(cudaMemcpy2DAsync(db, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
                              cudaMemcpyHostToDevice, s));
   int rc = refine_device_impl(p, db, p->n, dx, p->n, nrhs, tol, maxit, iters, resid, s);
@@ -1011,8 +1022,6 @@ int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int6
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
   }
-  cudaFree(db);
-  cudaFree(dx);
   return rc;
 }
 
