@@ -879,8 +879,8 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
 // The core lives in shared memory when it fits (RECOMP_SMEM_CORE doubles).
 // ---------------------------------------------------------------------------
 constexpr int RECOMP_THREADS = 512;
-constexpr int SPLIT_P = 48;       // split band-1 targets whose operand rank exceeds this
-constexpr int SPLIT_MAX = 32;     // band-1 tasks eligible for the split (scratch slots)
+constexpr int SPLIT_P = 32;       // split band-1 targets whose operand rank exceeds this
+constexpr int SPLIT_MAX = 128;    // band-1 tasks eligible for the split (scratch slots)
 constexpr int RECOMP_SMEM_BYTES = 227 * 1024 - 512;     // dynamic shared memory (all but the static part)
 constexpr int RECOMP_GSM = 2 * 16 * 64;                 // cta_gemm tiles (doubles)
 constexpr int RECOMP_REGION = RECOMP_SMEM_BYTES / 8 - RECOMP_GSM;  // doubles for panels / core
