@@ -941,11 +941,33 @@ int frank_blr_solve_transpose_device(frank_blr* p, double* d_b, int64_t ldb, int
   return FRANK_OK;
 }
 
+// Device copies for the host-buffer entry points (b, x or y): kept by the
+// plan and grown on demand, so that repeated calls do not allocate.  Returns
+// two n x nrhs regions.
+namespace {
+int host_io(frank_blr* p, int nrhs, double** a, double** b) {
+  const size_t need = (size_t)p->n * nrhs;
+  if (need > p->host_io_cap) {
+    if (p->host_io) cudaFree(p->host_io);
+    p->host_io = nullptr;
+    p->host_io_cap = 0;
+    CUDA_TRY(cudaMalloc(&p->host_io, 2 * need * sizeof(double)));
+    p->host_io_cap = need;
+  }
+  *a = p->host_io;
+  *b = p->host_io + need;
+  return FRANK_OK;
+}
+}  // namespace
+
 int frank_blr_solve(frank_blr* p, double* b, int64_t ldb, int nrhs, void* stream) {
   if (!p || !b || nrhs < 1 || ldb < p->n) return fail(FRANK_ERR_INVALID, "bad solve arguments");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  double* d = nullptr;
-  CUDA_TRY(cudaMalloc(&d, sizeof(double) * p->n * nrhs));
+  double *d = nullptr, *unused = nullptr;
+  {
+    const int rc0 = host_io(p, nrhs, &d, &unused);
+    if (rc0) return rc0;
+  }
   CUDA_TRY(cudaMemcpy2DAsync(d, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
                              cudaMemcpyHostToDevice, s));
   int rc = solve_device_impl(p, d, p->n, nrhs, false, s);
@@ -955,7 +977,6 @@ int frank_blr_solve(frank_blr* p, double* b, int64_t ldb, int nrhs, void* stream
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
   }
-  cudaFree(d);
   return rc;
 }
 
@@ -973,8 +994,10 @@ int frank_blr_matvec(frank_blr* p, const double* x, int64_t ldx, double* y, int6
   if (!p || !x || !y || nrhs < 1 || ldx < p->n || ldy < p->n) return fail(FRANK_ERR_INVALID, "bad matvec arguments");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double *dx = nullptr, *dy = nullptr;
-  CUDA_TRY(cudaMalloc(&dx, sizeof(double) * p->n * nrhs));
-  CUDA_TRY(cudaMalloc(&dy, sizeof(double) * p->n * nrhs));
+  {
+    const int rc0 = host_io(p, nrhs, &dx, &dy);
+    if (rc0) return rc0;
+  }
   CUDA_TRY(cudaMemcpy2DAsync(dx, p->n * sizeof(double), x, ldx * sizeof(double), p->n * sizeof(double), nrhs,
                              cudaMemcpyHostToDevice, s));
   int rc = matvec_device_impl(p, dx, p->n, dy, p->n, nrhs, nullptr, 0, s);
@@ -984,8 +1007,6 @@ int frank_blr_matvec(frank_blr* p, const double* x, int64_t ldx, double* y, int6
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
   }
-  cudaFree(dx);
-  cudaFree(dy);
   return rc;
 }
 
@@ -1001,18 +1022,11 @@ int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int6
   if (!p || !b || !x || nrhs < 1 || ldb < p->n || ldx < p->n || maxit < 0)
     return fail(FRANK_ERR_INVALID, "bad refine arguments");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // device copies of b and x: kept by the plan and grown on demand, so that
-  // repeated solves do not allocate
-  const size_t need = (size_t)p->n * nrhs;
-  if (need > p->host_io_cap) {
-    if (p->host_io) cudaFree(p->host_io);
-    p->host_io = nullptr;
-    p->host_io_cap = 0;
-    CUDA_TRY(cudaMalloc(&p->host_io, 2 * need * sizeof(double)));
-    p->host_io_cap = need;
+  double *db = nullptr, *dx = nullptr;
+  {
+    const int rc0 = host_io(p, nrhs, &db, &dx);
+    if (rc0) return rc0;
   }
-  double* db = p->host_io;
-  double* dx = p->host_io + need;
   CUDA_TRY(cudaMemcpy2DAsync(db, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
                              cudaMemcpyHostToDevice, s));
   int rc = refine_device_impl(p, db, p->n, dx, p->n, nrhs, tol, maxit, iters, resid, s);
