@@ -64,6 +64,7 @@ struct frank_blr {
   double* host_io = nullptr;    // device copies of b and x for frank_blr_refine
   size_t host_io_cap = 0;
   int* split_done = nullptr;    // [nb][SPLIT_MAX] side counters
+  int nsplit = 0;               // split slots allocated
   int64_t dstride = 0, rstride = 0;
   int grid_dense = 0, grid_recomp = 0, smax = 0;
   int core_method = CORE_RRQR;
@@ -167,8 +168,18 @@ bool split_on(const frank_blr* p) { return p->nb > 2 && p->grid_recomp >= p->sm_
 int ensure_scratch(frank_blr* p) {
   if (!p->dscratch) CUDA_TRY(dalloc(&p->dscratch, (size_t)p->grid_dense * p->dstride));
   if (p->nlr > 0 && split_on(p) && !p->rsplit) {
-    CUDA_TRY(dalloc(&p->rsplit, (size_t)SPLIT_MAX * p->rstride));
-    CUDA_TRY(dalloc(&p->split_done, (size_t)p->nb * SPLIT_MAX));
+    // one slot per band-1 task of the first step (at most SPLIT_MAX); the
+    // split is an optimisation, so without the memory the plan runs without it
+    p->nsplit = std::min(SPLIT_MAX, 2 * (p->nb - 2));
+    if (dalloc(&p->rsplit, (size_t)p->nsplit * p->rstride) != cudaSuccess ||
+        dalloc(&p->split_done, (size_t)p->nb * SPLIT_MAX) != cudaSuccess) {
+      cudaGetLastError();
+      if (p->rsplit) cudaFree(p->rsplit);
+      if (p->split_done) cudaFree(p->split_done);
+      p->rsplit = nullptr;
+      p->split_done = nullptr;
+      p->nsplit = 0;
+    }
   }
   if (p->nlr > 0 && !p->rscratch)
     CUDA_TRY(dalloc(&p->rscratch, (size_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
@@ -281,7 +292,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
             W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0, p->work + i,
-            p->rsplit ? SPLIT_MAX : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr);
+            p->rsplit ? p->nsplit : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr);
         ++launches;
       }
     }
