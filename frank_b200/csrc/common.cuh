@@ -615,18 +615,19 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
     if (lane == 0) { cnorm[c] = sqrt(s); partial[c] = sqrt(s); jpvt[c] = c; }
   }
   __syncthreads();
+  // the arg-max of the remaining column norms serves both the stopping test
+  // and the next pivot (the norms do not change in between)
   double maxc;
+  int kp_next;
   {
     double best = -1.0; int bi = -1;
     for (int c = threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
-    block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+    kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
   }
   int r = 0;
   while (r < mind && maxc > thr) {
     double best = -1.0; int bi = -1;
-    for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
-    double dummy;
-    const int kp = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &dummy);
+    const int kp = kp_next;
     if (kp != r) {
       for (int e = threadIdx.x; e < m; e += blockDim.x) {
         const double a = A[e + (int64_t)r * lda];
@@ -689,7 +690,7 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
     ++r;
     best = -1.0; bi = -1;
     for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
-    block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+    kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
     if (r >= n) maxc = 0.0;
   }
   __syncthreads();
