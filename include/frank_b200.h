@@ -155,7 +155,11 @@ int frank_blr_getrf(frank_blr* plan, void* stream);
 
 /* x = U^{-1} L^{-1} P b for nrhs right-hand sides (column-major n x nrhs,
  * leading dimension ldb), in place.  Replaces trsm(L, b, Lower) followed by
- * trsm(U, b, Upper) (trsm.cpp:117-125, 40-90; examples/h_lu.cpp:45-48). */
+ * trsm(U, b, Upper) (trsm.cpp:117-125, 40-90; examples/h_lu.cpp:45-48).
+ * The host-buffer calls (frank_blr_solve, frank_blr_matvec, frank_blr_refine)
+ * stage b, x and y in one device buffer owned by the plan (allocated at the
+ * first call, grown when nrhs grows), so calls on the same plan must not
+ * overlap; the _device variants use only the caller's buffers. */
 int frank_blr_solve(frank_blr* plan, double* b, int64_t ldb, int nrhs, void* stream);
 int frank_blr_solve_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
 
