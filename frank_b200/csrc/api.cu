@@ -39,6 +39,18 @@ cudaError_t dalloc(P** p, size_t count) {
   return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(P));
 }
 
+// Device allocation owned by a scope: freed on every return path.
+template <typename P>
+struct DevBuf {
+  P* ptr = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (ptr) cudaFree(ptr); }
+  cudaError_t alloc(size_t count) { return dalloc(&ptr, count); }
+  P* get() const { return ptr; }
+};
+
 }  // namespace
 
 struct frank_blr {
@@ -750,27 +762,29 @@ int frank_blr_build_kernel(frank_blr* p, int kernel, const double* points, int d
   if (kernel < 0 || kernel > 3 || dim < 1 || dim > 3) return fail(FRANK_ERR_INVALID, "bad kernel or dim");
   if (eps <= 0.0 && p->fixed_rank <= 0)
     return fail(FRANK_ERR_UNSUPPORTED, "on-device construction needs eps > 0 or a fixed-rank plan");
+  if (kernel == FRANK_KERNEL_EXP && !(kparams && kparams[0] > 0.0))
+    return fail(FRANK_ERR_INVALID, "exp kernel needs theta > 0");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  double* dx = nullptr;
-  CUDA_TRY(cudaMalloc(&dx, sizeof(double) * dim * p->n));
-  CUDA_TRY(cudaMemcpy(dx, points, sizeof(double) * dim * p->n, cudaMemcpyHostToDevice));
+  // construction temporaries: freed on every return path
+  DevBuf<double> dx, d_of, d_ol, scratch;
+  DevBuf<int> d_dl, d_ll;
+  CUDA_TRY(dx.alloc((size_t)dim * p->n));
+  CUDA_TRY(cudaMemcpy(dx.get(), points, sizeof(double) * dim * p->n, cudaMemcpyHostToDevice));
   KernelDesc K;
-  K.kind = kernel; K.dim = dim; K.x = dx; K.n = p->n;
+  K.kind = kernel; K.dim = dim; K.x = dx.get(); K.n = p->n;
   K.p0 = kparams ? kparams[0] : 0.0;
   K.p1 = kparams ? kparams[1] : 0.0;
-  if (kernel == FRANK_KERNEL_EXP && !(K.p0 > 0.0)) { cudaFree(dx); return fail(FRANK_ERR_INVALID, "exp kernel needs theta > 0"); }
   std::vector<int> dl, ll;
   for (int b = 0; b < p->nb * p->nb; ++b) {
     if (p->dslot_h[b] >= 0) dl.push_back(b);
     else ll.push_back(b);
   }
-  int *d_dl = nullptr, *d_ll = nullptr;
-  CUDA_TRY(dalloc(&d_dl, dl.size()));
-  CUDA_TRY(dalloc(&d_ll, ll.size()));
-  if (!dl.empty()) CUDA_TRY(cudaMemcpy(d_dl, dl.data(), sizeof(int) * dl.size(), cudaMemcpyHostToDevice));
-  if (!ll.empty()) CUDA_TRY(cudaMemcpy(d_ll, ll.data(), sizeof(int) * ll.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(d_dl.alloc(dl.size()));
+  CUDA_TRY(d_ll.alloc(ll.size()));
+  if (!dl.empty()) CUDA_TRY(cudaMemcpy(d_dl.get(), dl.data(), sizeof(int) * dl.size(), cudaMemcpyHostToDevice));
+  if (!ll.empty()) CUDA_TRY(cudaMemcpy(d_ll.get(), ll.data(), sizeof(int) * ll.size(), cudaMemcpyHostToDevice));
   BlrView<double> H = h_view(p);
-  if (!dl.empty()) k_build_dense<<<(int)std::min<size_t>(dl.size(), 4096), 256, 0, s>>>(H, K, d_dl, (int)dl.size());
+  if (!dl.empty()) k_build_dense<<<(int)std::min<size_t>(dl.size(), 4096), 256, 0, s>>>(H, K, d_dl.get(), (int)dl.size());
   int rc = FRANK_OK;
   if (!ll.empty() && eps <= 0.0) {
     // fixed rank: LowRank(Dense, rank) -> rsvd with sample min(rank + 5, m, n)
@@ -778,10 +792,8 @@ int frank_blr_build_kernel(frank_blr* p, int kernel, const double* points, int d
     const int64_t bm = p->bmax;
     const int last = p->off_h[p->nb] - p->off_h[p->nb - 1];
     const int psamp = std::min<int>(p->fixed_rank + 5, std::min<int>(bm, last));
-    if (p->fixed_rank + 5 > last && last != bm) {
-      cudaFree(dx);
+    if (p->fixed_rank + 5 > last && last != bm)
       return fail(FRANK_ERR_UNSUPPORTED, "fixed-rank construction with a short last block below rank + 5");
-    }
     auto omega = [&](int ncols) {
       std::mt19937 gen;
       gen.seed(0);
@@ -791,42 +803,34 @@ int frank_blr_build_kernel(frank_blr* p, int kernel, const double* points, int d
       return om;
     };
     const std::vector<double> of = omega((int)bm), ol = omega(last);
-    double *d_of = nullptr, *d_ol = nullptr;
-    CUDA_TRY(cudaMalloc(&d_of, sizeof(double) * of.size()));
-    CUDA_TRY(cudaMalloc(&d_ol, sizeof(double) * ol.size()));
-    CUDA_TRY(cudaMemcpy(d_of, of.data(), sizeof(double) * of.size(), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(d_ol, ol.data(), sizeof(double) * ol.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(d_of.alloc(of.size()));
+    CUDA_TRY(d_ol.alloc(ol.size()));
+    CUDA_TRY(cudaMemcpy(d_of.get(), of.data(), sizeof(double) * of.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d_ol.get(), ol.data(), sizeof(double) * ol.size(), cudaMemcpyHostToDevice));
     const int64_t stride = bm * bm + 2 * bm * psamp + (bm + psamp) * psamp + 4 * psamp + 64;
     const int grid = (int)std::min<size_t>(ll.size(), (size_t)2 * p->sm_count);
-    double* scratch = nullptr;
-    CUDA_TRY(cudaMalloc(&scratch, sizeof(double) * stride * grid));
+    CUDA_TRY(scratch.alloc((size_t)stride * grid));
     CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
-    k_build_lowrank_rsvd<<<grid, BUILD_THREADS, 0, s>>>(H, K, d_ll, (int)ll.size(), p->fixed_rank, psamp, d_of, d_ol,
-                                                        stride, scratch, p->err);
+    k_build_lowrank_rsvd<<<grid, BUILD_THREADS, 0, s>>>(H, K, d_ll.get(), (int)ll.size(), p->fixed_rank, psamp,
+                                                        d_of.get(), d_ol.get(), stride, scratch.get(), p->err);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s));
     CUDA_TRY(cudaMemcpy(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost));
-    cudaFree(scratch); cudaFree(d_of); cudaFree(d_ol);
     if (p->err_h[ERR_RANK_OVERFLOW]) rc = fail(FRANK_ERR_RANK_OVERFLOW, "the fixed rank exceeds max_rank");
   } else if (!ll.empty()) {
     const int64_t bm = p->bmax;
     const int64_t stride = 3 * bm * bm + 6 * bm;
     const int grid = (int)std::min<size_t>(ll.size(), (size_t)2 * p->sm_count);
-    double* scratch = nullptr;
-    CUDA_TRY(cudaMalloc(&scratch, sizeof(double) * stride * grid));
+    CUDA_TRY(scratch.alloc((size_t)stride * grid));
     CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
-    k_build_lowrank<<<grid, BUILD_THREADS, 0, s>>>(H, K, d_ll, (int)ll.size(), eps, scratch, stride, p->err);
+    k_build_lowrank<<<grid, BUILD_THREADS, 0, s>>>(H, K, d_ll.get(), (int)ll.size(), eps, scratch.get(), stride, p->err);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s));
     CUDA_TRY(cudaMemcpy(p->err_h, p->err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost));
-    cudaFree(scratch);
     if (p->err_h[ERR_RANK_OVERFLOW]) rc = fail(FRANK_ERR_RANK_OVERFLOW, "a compressed block exceeded max_rank and was truncated");
   }
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(s));
-  cudaFree(dx);
-  if (d_dl) cudaFree(d_dl);
-  if (d_ll) cudaFree(d_ll);
   p->factored = false;
   return rc;
 }
@@ -1101,15 +1105,18 @@ extern "C" int frank_kernel_dtheta_contract(int kernel, const double* d_points, 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int64_t tiles = (n + DT_TILE - 1) / DT_TILE;
   if (tiles > 65535) return fail(FRANK_ERR_UNSUPPORTED, "too many points for the contraction grid");
+  // per-tile partials from the stream-ordered pool (no device-wide
+  // synchronisation, reused across calls by the pool)
   double* part = nullptr;
-  CUDA_TRY(cudaMalloc(&part, sizeof(double) * tiles * tiles));
+  CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * tiles * tiles, s));
   k_dtheta_contract<<<dim3((unsigned)tiles, (unsigned)tiles), 256, 0, s>>>(d_points, dim, n, kparams[0], d_lambda, ldl,
                                                                           d_x, ldx, nrhs, part);
   cudaError_t e = cudaGetLastError();
   std::vector<double> h((size_t)tiles * tiles);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s);
+  cudaError_t ef = cudaFreeAsync(part, s);
+  if (e == cudaSuccess) e = ef;
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cudaFree(part);
   if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
   double acc = 0.0;
   for (double v : h) acc += v;
@@ -1390,23 +1397,71 @@ __global__ void k_noalloc_pivots(int n, int* out) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) out[r] = ip[r] + 1;
 }
 
-// Device address of the scratch, looked up once per device (the host-side
-// name of a __device__ array is not a device address).
+// Device address of the scratch, looked up once per device context (the
+// host-side name of a __device__ array is not a device address).  The entry
+// is keyed by the driver's unique id of the current context, so a context
+// created after cudaDeviceReset (where the module, and with it the array, is
+// loaded afresh) triggers a new lookup instead of reusing a stale address.
 constexpr int NA_MAX_DEVICES = 64;
-unsigned char* g_noalloc_addr[NA_MAX_DEVICES] = {nullptr};
+struct NoallocEntry {
+  unsigned char* addr = nullptr;
+  unsigned long long ctx_id = 0;
+};
+NoallocEntry g_noalloc_addr[NA_MAX_DEVICES];
 std::mutex g_noalloc_mutex;
+
+// Unique id of the calling thread's current context (cuCtxGetCurrent +
+// cuCtxGetId, reached through the runtime's driver entry-point query so the
+// library does not link libcuda); 0 when the driver does not provide it.
+unsigned long long current_context_id() {
+  using GetCurrentFn = int (*)(void**);
+  using GetIdFn = int (*)(void*, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetIdFn>(f);
+    cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 int noalloc_setup(int dev, unsigned char** out) {
   if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(FRANK_ERR_UNSUPPORTED, "device index beyond the set-up table");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_addr[dev]) {
+  // A thread that has not used the runtime yet has no current context (id 0):
+  // the lookup below makes the device's primary context current, and the id
+  // is read again after it.
+  const unsigned long long ctx = current_context_id();
+  NoallocEntry& slot = g_noalloc_addr[dev];
+  if (!slot.addr || ctx == 0 || slot.ctx_id != ctx) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr)
       return fail(FRANK_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-    g_noalloc_addr[dev] = static_cast<unsigned char*>(ptr);
+    // Under lazy module loading a kernel is loaded at its first launch, which
+    // may allocate device memory; load the three kernels of this entry point
+    // here, at set-up, so later calls load nothing.
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k_noalloc_prepare));
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k_getrf<double>));
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k_noalloc_pivots));
+    slot.addr = static_cast<unsigned char*>(ptr);
+    slot.ctx_id = current_context_id();
   }
-  *out = g_noalloc_addr[dev];
+  *out = slot.addr;
   return FRANK_OK;
 }
 

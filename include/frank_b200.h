@@ -156,10 +156,13 @@ int frank_blr_getrf(frank_blr* plan, void* stream);
 /* x = U^{-1} L^{-1} P b for nrhs right-hand sides (column-major n x nrhs,
  * leading dimension ldb), in place.  Replaces trsm(L, b, Lower) followed by
  * trsm(U, b, Upper) (trsm.cpp:117-125, 40-90; examples/h_lu.cpp:45-48).
- * The host-buffer calls (frank_blr_solve, frank_blr_matvec, frank_blr_refine)
- * stage b, x and y in one device buffer owned by the plan (allocated at the
- * first call, grown when nrhs grows), so calls on the same plan must not
- * overlap; the _device variants use only the caller's buffers. */
+ * Every call on a plan (solve, matvec, refine, their _device and transposed
+ * variants) writes plan-owned device workspace (the FP32 solve vector of a
+ * mixed plan, the matvec partials, the refinement residual), so calls on the
+ * same plan must be serialised.  The host-buffer calls (frank_blr_solve,
+ * frank_blr_matvec, frank_blr_refine) additionally stage b, x and y in one
+ * device buffer owned by the plan (allocated at the first call, grown when
+ * nrhs grows); the _device variants only avoid that staging buffer. */
 int frank_blr_solve(frank_blr* plan, double* b, int64_t ldb, int nrhs, void* stream);
 int frank_blr_solve_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
 
@@ -261,10 +264,16 @@ int frank_blr_kernel_times(const frank_blr* plan, double* ms, double* flops);
  * The scratch is one fixed 2 MB array in device memory (a file-scope
  * __device__ array of the library) that every GPU loading the library holds
  * until exit; all calls share it and it keeps the last call's contents.  The
- * first call on a device looks up the array's device address (set-up, once
- * per device); make that first call before any stream capture.  The call is
- * synchronous on `stream`.  Calls that overlap on the GPU (from several host
- * threads or streams at once) race on the shared scratch: serialise them. */
+ * first call on a device (and the first after the device's context has been
+ * re-created, e.g. by cudaDeviceReset) does the set-up: it looks up the
+ * array's device address and loads this entry point's kernels.  With CUDA's
+ * default lazy module loading that loading can itself take device memory, so
+ * make one warm-up call per device at start-up, while memory is still
+ * available; later calls load and allocate nothing.  The call synchronises
+ * `stream` and reads status words back to the host, so it cannot be made
+ * inside a stream capture at all.  Calls that overlap on the GPU (from
+ * several host threads or streams at once) race on the shared scratch:
+ * serialise them. */
 int frank_getrf_dense_noalloc(const double* d_a, int64_t lda, int n, double* d_lu, int64_t ldlu,
                               int* d_ipiv, void* stream);
 

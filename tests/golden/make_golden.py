@@ -1,5 +1,7 @@
-"""Regenerate the golden fixtures of tests/golden (run in a container that has
-the FRANK sources; the fixtures are committed so the tests never need them).
+"""Regenerate the golden fixtures of tests/golden (run where the FRANK sources
+are available; the fixtures are committed so the tests never need them).
+
+Usage: python tests/golden/make_golden.py --reference <FRANK checkout> [--workdir <dir>]
 
 1. libstdcxx_mt19937_seed0.txt: raw std::mt19937(0) outputs and libstdc++
    uniform_real_distribution / normal_distribution draws, printed by
@@ -11,26 +13,27 @@ the FRANK sources; the fixtures are committed so the tests never need them).
    (functions.py laplace1d) with the dense_getrf_test diagonal boost
    (test/dense_getrf_test.cpp:25-30), n = 8, 16, 32.
 """
+import argparse
 import os
 import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_PY = "/root/reference/python"
 
 
-def make_rng():
-    exe = os.path.join("/tmp", "gen_libstdcxx_mt19937")
+def make_rng(workdir):
+    exe = os.path.join(workdir, "gen_libstdcxx_mt19937")
     subprocess.check_call(["g++", "-O2", os.path.join(HERE, "gen_libstdcxx_mt19937.cpp"), "-o", exe])
     out = subprocess.check_output([exe]).decode()
     with open(os.path.join(HERE, "libstdcxx_mt19937_seed0.txt"), "w") as f:
         f.write(out)
 
 
-def make_prototype_lu():
-    sys.path.insert(0, REF_PY)
+def make_prototype_lu(reference):
+    sys.path.insert(0, os.path.join(reference, "python"))
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     from FRANK.dense import Dense            # reference prototype
     from FRANK.functions import laplace1d
@@ -54,6 +57,11 @@ def make_prototype_lu():
 
 
 if __name__ == "__main__":
-    make_rng()
-    make_prototype_lu()
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True, help="FRANK source tree (its python/ prototype is imported)")
+    ap.add_argument("--workdir", default=None, help="scratch directory for the compiled RNG probe")
+    args = ap.parse_args()
+    with tempfile.TemporaryDirectory(dir=args.workdir) as wd:
+        make_rng(wd)
+    make_prototype_lu(args.reference)
     print("ok")
