@@ -1,10 +1,11 @@
 """Benchmark: BLR-LU factor + solve time to a 1e-10 residual, mixed vs plain FP64.
 
 Workload (the headline configuration): Laplace-3D kernel 1/(r + 1e-3) on
-N = 32768 uniform points in the unit cube (numpy PCG64 seed 2), Morton
-ordered (morton_index.cpp rule), BLR with 64 x 64 blocks of 512, weak
-admissibility, A_H compressed on the device to eps = 1e-8, 4 right-hand
-sides b ~ N(0, 1) (seed 3), target max_j ||b_j - A_H x_j|| / ||b_j|| <= 1e-10.
+N = 32768 uniform points in the unit cube (std::mt19937_64 seed 2, drawn
+axis-major), Morton ordered (morton_index.cpp rule), BLR with 64 x 64 blocks
+of 512, weak admissibility, A_H compressed on the device to eps = 1e-8, 4
+right-hand sides b ~ N(0, 1) (std::mt19937_64 seed 3, column by column),
+target max_j ||b_j - A_H x_j|| / ||b_j|| <= 1e-10.
 
 One step = getrf (the FP32 factor at tolerance 3e-3 for "mixed", the FP64
 factor at 1e-8 for "fp64") + iterative refinement against the FP64 A_H to
@@ -40,12 +41,108 @@ CFG = dict(n=32768, nb=64, dim=3, eps=1e-8, mixed_eps=3e-3, nrhs=4, tol=1e-10, k
            point_seed=2, rhs_seed=3, morton_level=10)
 
 
+class MT19937_64:
+    """std::mt19937_64 seeded with `gen.seed(s)` (Matsumoto-Nishimura 64-bit
+    Mersenne Twister: n = 312, m = 156, init multiplier 6364136223846793005),
+    with libstdc++'s uniform_real_distribution<double>(0, 1) (one 64-bit draw
+    per variate: double(g) / 2^64, clamped below 1) and
+    normal_distribution<double>(0, 1) (Marsaglia polar method, the second
+    variate of each accepted pair returned by the next call).  Pinned against
+    g++ output in tests/golden/libstdcxx_mt19937_seed0.txt."""
+
+    N, M = 312, 156
+    A = 0xB5026F5AA96619E9
+    UM, LM = 0xFFFFFFFF80000000, 0x7FFFFFFF
+
+    def __init__(self, seed):
+        import numpy as np
+        mt = [seed & 0xFFFFFFFFFFFFFFFF]
+        for i in range(1, self.N):
+            mt.append((6364136223846793005 * (mt[-1] ^ (mt[-1] >> 62)) + i) & 0xFFFFFFFFFFFFFFFF)
+        self.mt = np.array(mt, dtype=np.uint64)
+        self.pos = self.N
+        self.pending = np.empty(0, dtype=np.uint64)   # drawn but not consumed
+        self.saved = None                               # cached second normal variate
+
+    def _twist(self):
+        import numpy as np
+        mt, A, UM, LM = self.mt, np.uint64(self.A), np.uint64(self.UM), np.uint64(self.LM)
+        one = np.uint64(1)
+        y = (mt[0:156] & UM) | (mt[1:157] & LM)
+        mt[0:156] = mt[156:312] ^ (y >> one) ^ ((y & one) * A)
+        y = (mt[156:311] & UM) | (mt[157:312] & LM)
+        mt[156:311] = mt[0:155] ^ (y >> one) ^ ((y & one) * A)
+        y = (mt[311] & UM) | (mt[0] & LM)
+        mt[311] = mt[155] ^ (y >> one) ^ ((y & one) * A)
+        self.pos = 0
+
+    def raw(self, count):
+        import numpy as np
+        out = np.empty(count, dtype=np.uint64)
+        k = min(count, len(self.pending))
+        out[:k] = self.pending[:k]
+        self.pending = self.pending[k:]
+        while k < count:
+            if self.pos >= self.N:
+                self._twist()
+            take = min(count - k, self.N - self.pos)
+            x = self.mt[self.pos:self.pos + take].copy()
+            x ^= (x >> np.uint64(29)) & np.uint64(0x5555555555555555)
+            x ^= (x << np.uint64(17)) & np.uint64(0x71D67FFFEDA60000)
+            x ^= (x << np.uint64(37)) & np.uint64(0xFFF7EEE000000000)
+            x ^= x >> np.uint64(43)
+            out[k:k + take] = x
+            self.pos += take
+            k += take
+        return out
+
+    def uniform(self, count):
+        import numpy as np
+        return self._canonical(self.raw(count))
+
+    @staticmethod
+    def _canonical(r):
+        import numpy as np
+        u = r.astype(np.float64) / 18446744073709551616.0
+        u[u >= 1.0] = np.nextafter(1.0, 0.0)
+        return u
+
+    def normal(self, count):
+        import numpy as np
+        out = []
+        if count > 0 and self.saved is not None:
+            out.append(self.saved)
+            self.saved = None
+        while len(out) < count:
+            pairs = int((count - len(out)) * 0.7) + 16
+            r = self.raw(2 * pairs)
+            u = self._canonical(r)
+            x, y = 2.0 * u[0::2] - 1.0, 2.0 * u[1::2] - 1.0
+            r2 = x * x + y * y
+            acc = np.nonzero(~((r2 > 1.0) | (r2 == 0.0)))[0]
+            use = acc[: (count - len(out) + 1) // 2]
+            if len(use) == 0:
+                continue
+            last = int(use[-1])
+            self.pending = np.concatenate([r[2 * (last + 1):], self.pending])   # draws not consumed
+            mult = np.sqrt(-2.0 * np.log(r2[use]) / r2[use])
+            pv = np.empty(2 * len(use))
+            pv[0::2] = y[use] * mult
+            pv[1::2] = x[use] * mult
+            out.extend(pv.tolist())
+        if len(out) > count:
+            self.saved = out[count]
+        return np.array(out[:count])
+
+
 def make_points(n, dim, seed, level):
+    """n points uniform in [0, 1)^dim from std::mt19937_64 seeded `seed`,
+    drawn axis-major (all x, then all y, ...; the reference's params[d][i]
+    layout, functions.h:34-38), then Morton ordered
+    (operations/misc/morton_index.cpp:36-98): the bounding box padded by 0.5,
+    `level` bits interleaved per axis, stable sort by box number."""
     import numpy as np
-    rng = np.random.default_rng(seed)
-    x = rng.random((dim, n))
-    # Morton order (operations/misc/morton_index.cpp:36-98): pad the bounding
-    # box by 0.5, interleave `level` bits per axis, stable sort by box number.
+    x = MT19937_64(seed).uniform(dim * n).reshape(dim, n)
     bmin = x.min(axis=1) - 0.5
     bsize = float((x.max(axis=1) - x.min(axis=1)).max()) + 1.0
     ix = (((x - bmin[:, None]) / bsize) * (1 << level)).astype(np.int64)
@@ -55,6 +152,13 @@ def make_points(n, dim, seed, level):
             code += (ix[d] & 1) << (dim * lev + d)
             ix[d] >>= 1
     return x[:, np.argsort(code, kind="stable")].copy()
+
+
+def make_rhs(n, nrhs, seed):
+    """n x nrhs right-hand sides b ~ N(0, 1) from std::mt19937_64 seeded
+    `seed`, column by column (Fortran order)."""
+    import numpy as np
+    return np.asfortranarray(MT19937_64(seed).normal(n * nrhs).reshape(nrhs, n).T)
 
 
 class Clocks:
@@ -138,8 +242,7 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     c = CFG
     x = make_points(c["n"], c["dim"], c["point_seed"] + rank, c["morton_level"])
-    rng = np.random.default_rng(c["rhs_seed"] + rank)
-    b_host = np.asfortranarray(rng.standard_normal((c["n"], c["nrhs"])))
+    b_host = make_rhs(c["n"], c["nrhs"], c["rhs_seed"] + rank)
     b_dev = torch.from_numpy(b_host.T.copy()).to("cuda")          # (nrhs, n) row-major == column-major n x nrhs
     x_dev = torch.zeros_like(b_dev)
     stream = torch.cuda.current_stream().cuda_stream

@@ -11,11 +11,13 @@ import oracle.frank_oracle as fo
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def _gold_rng():
+def _gold_rng(suffix=""):
     raw, uni, nor = [], [], []
     for line in open(os.path.join(GOLD, "libstdcxx_mt19937_seed0.txt")):
         k, v = line.split()
-        {"raw": raw, "uniform": uni, "normal": nor}[k].append(float(v))
+        d = {"raw" + suffix: raw, "uniform" + suffix: uni, "normal" + suffix: nor}.get(k)
+        if d is not None:
+            d.append(int(v) if k.startswith("raw") else float(v))
     return raw, uni, nor
 
 
@@ -24,6 +26,19 @@ def test_mt19937_streams_match_libstdcxx():
     assert list(fo.StdMT19937(0).raw(len(raw))) == [int(v) for v in raw]
     np.testing.assert_array_equal(fo.StdMT19937(0).uniform(len(uni)), np.array(uni))
     np.testing.assert_allclose(fo.StdMT19937(0).normal(len(nor)), np.array(nor), rtol=0, atol=1e-15)
+
+
+def test_mt19937_64_streams_match_libstdcxx():
+    """The benchmark's input streams (std::mt19937_64 seeded 2 for points, 3
+    for right-hand sides) against g++ output."""
+    from bench import MT19937_64
+    raw, uni, nor = _gold_rng("64")
+    assert [int(v) for v in MT19937_64(2).raw(len(raw))] == raw
+    np.testing.assert_array_equal(MT19937_64(2).uniform(len(uni)), np.array(uni))
+    np.testing.assert_allclose(MT19937_64(3).normal(len(nor)), np.array(nor), rtol=0, atol=1e-15)
+    g = MT19937_64(3)          # drawn in pieces: the cached second variate carries over
+    pieces = np.concatenate([g.normal(101), g.normal(300), g.normal(len(nor) - 401)])
+    np.testing.assert_allclose(pieces, np.array(nor), rtol=0, atol=1e-15)
 
 
 def test_prototype_dense_lu_fixture():
