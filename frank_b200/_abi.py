@@ -46,6 +46,7 @@ SIGNATURES = {
     "frank_last_error": (C.c_char_p, []),
     "frank_device_info": (C.c_int, [C.c_char_p, C.c_int, _ip, _ip, _ip]),
     "frank_blr_create": (C.c_int, [C.POINTER(BlrDesc), C.POINTER(_vp)]),
+    "frank_blr_create_geometric": (C.c_int, [C.POINTER(BlrDesc), _dp, C.c_int, C.POINTER(_vp)]),
     "frank_blr_destroy": (C.c_int, [_vp]),
     "frank_blr_offsets": (C.c_int, [_vp, _i64p]),
     "frank_blr_set_dense": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_int64, C.c_int]),

@@ -47,16 +47,29 @@ class BLRMatrix:
     |i - j| > admis (position-based admissibility, matrix_initializer.cpp:51-58)."""
 
     def __init__(self, n: int, nb: int, *, eps: float = 0.0, fixed_rank: int = 0, max_rank: int = 0,
-                 precision: str = "fp64", admis: float = 0.0):
+                 precision: str = "fp64", admis: float = 0.0, admis_type: str = "position",
+                 points: Optional[np.ndarray] = None):
+        """admis_type "position": block (i, j) low rank iff |i - j| > admis;
+        "geometry": from the bounding boxes of `points` (dim x n), as
+        AdmisType::GeometryBased (matrix_initializer.cpp:51-91)."""
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
+        if admis_type not in ("position", "geometry"):
+            raise ValueError("admis_type must be 'position' or 'geometry'")
         self.n, self.nb = int(n), int(nb)
         self.precision = precision
         d = _abi.BlrDesc(n=self.n, nb=self.nb, max_rank=int(max_rank),
                          precision=_abi.FRANK_PREC_FP64 if precision == "fp64" else _abi.FRANK_PREC_MIXED,
                          fixed_rank=int(fixed_rank), eps=float(eps), admis=float(admis))
         h = C.c_void_p()
-        check(lib().frank_blr_create(C.byref(d), C.byref(h)), "frank_blr_create")
+        if admis_type == "geometry":
+            if points is None:
+                raise ValueError("geometry-based admissibility needs points")
+            x = np.ascontiguousarray(np.atleast_2d(points), dtype=np.float64)
+            check(lib().frank_blr_create_geometric(C.byref(d), _dptr(x), x.shape[0], C.byref(h)),
+                  "frank_blr_create_geometric")
+        else:
+            check(lib().frank_blr_create(C.byref(d), C.byref(h)), "frank_blr_create")
         self._h = h
         off = np.zeros(self.nb + 1, dtype=np.int64)
         check(lib().frank_blr_offsets(self._h, off.ctypes.data_as(C.POINTER(C.c_int64))), "frank_blr_offsets")
@@ -150,8 +163,10 @@ class BLRMatrix:
 
     # -- the path -----------------------------------------------------------
     def set_lra(self, name: str, core_scale: float = 0.1):
-        """FRANK_LRA: "rounded_addition" (core SVD, the reference algorithm) or
-        "rounded_addition_rrqr" (truncated_geqp3 + rq of the core, default)."""
+        """FRANK_LRA: "rounded_addition" (core SVD, the reference algorithm),
+        "fast_rounded_addition" (default of fixed-rank plans; tolerance plans
+        fall back to rounded_addition) or "rounded_addition_rrqr"
+        (truncated_geqp3 + rq of the core, default of tolerance plans)."""
         check(lib().frank_blr_set_lra(self._h, name.encode(), float(core_scale)), "frank_blr_set_lra")
 
     def getrf(self, stream: Optional[int] = None, allow=()):
@@ -233,6 +248,8 @@ def upload_hierarchical(H, n: int, nb: int, **kw) -> BLRMatrix:
     for i in range(nb):
         for j in range(nb):
             blk = H[i][j]
+            if isinstance(blk, np.ndarray) and A.is_lowrank(i, j):
+                raise ValueError("block (%d, %d) is dense but low rank under the plan's admissibility" % (i, j))
             if isinstance(blk, np.ndarray):
                 A.set_dense(i, j, blk)
             else:

@@ -79,7 +79,8 @@ struct frank_blr {
   int nsplit = 0;               // split slots allocated
   int64_t dstride = 0, rstride = 0;
   int grid_dense = 0, grid_recomp = 0, smax = 0;
-  int core_method = CORE_RRQR;
+  int core_method = CORE_RRQR;   // core of tolerance plans
+  int core_fixed = CORE_FAST;    // core of fixed-rank plans (FRANK_LRA unset: fast_rounded_addition)
   double core_scale = 0.1;
   int grid_gram = 0;
   double gram_tol = 1e-12;
@@ -303,7 +304,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
         }
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-            W, ws, i, p->smax, p->fixed_rank > 0 ? CORE_SVD : p->core_method, p->core_scale, 0, p->work + i,
+            W, ws, i, p->smax, p->fixed_rank > 0 ? p->core_fixed : p->core_method, p->core_scale, 0, p->work + i,
             p->rsplit ? p->nsplit : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr);
         ++launches;
       }
@@ -561,7 +562,41 @@ int frank_device_info(char* name, int name_len, int* sm_count, int* cc_major, in
   return FRANK_OK;
 }
 
-int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
+namespace {
+// Block (i, j) of a geometry-based plan is admissible when admis^2 diam^2 <
+// dist^2 for the bounding boxes of its row and column points, each padded by
+// 0.5 (classes/initialization_helpers/matrix_initializer.cpp:51-91).
+bool geometry_admissible(const double* x, int dim, int64_t n, int64_t r0, int64_t rn, int64_t c0, int64_t cn,
+                         double admis) {
+  const double off = 0.5;
+  double len_r = 0.0, len_c = 0.0, dist = 0.0;
+  for (int d = 0; d < dim; ++d) {
+    const double* ax = x + (int64_t)d * n;
+    const double rmin = *std::min_element(ax + r0, ax + r0 + rn) - off, rmax = *std::max_element(ax + r0, ax + r0 + rn) + off;
+    const double cmin = *std::min_element(ax + c0, ax + c0 + cn) - off, cmax = *std::max_element(ax + c0, ax + c0 + cn) + off;
+    len_r = std::max(len_r, rmax - rmin);
+    len_c = std::max(len_c, cmax - cmin);
+    const double dc = std::fabs((rmin + (rmax - rmin) / 2.0) - (cmin + (cmax - cmin) / 2.0));
+    dist += dc * dc;
+  }
+  const double diam = std::max(len_r, len_c);
+  return admis * admis * diam * diam < dist;
+}
+
+int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_blr** out);
+}  // namespace
+
+int frank_blr_create(const frank_blr_desc* d, frank_blr** out) { return create_impl(d, nullptr, 0, out); }
+
+int frank_blr_create_geometric(const frank_blr_desc* d, const double* points, int dim, frank_blr** out) {
+  if (!points || dim < 1 || dim > 3) return fail(FRANK_ERR_INVALID, "geometry-based admissibility needs points, dim 1..3");
+  return create_impl(d, points, dim, out);
+}
+
+}  // extern "C"
+
+namespace {
+int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_blr** out) {
   if (!d || !out) return fail(FRANK_ERR_INVALID, "null descriptor");
   *out = nullptr;
   if (d->n <= 0 || d->nb <= 0 || d->nb > d->n) return fail(FRANK_ERR_INVALID, "need 0 < nb <= n");
@@ -589,7 +624,9 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   for (int i = 0; i < nb; ++i)
     for (int j = 0; j < nb; ++j) {
       const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j];
-      const bool adm = (i != j) && (std::abs(i - j) > (int)d->admis) && bi > 1 && bj > 1;
+      const bool adm = (i != j) && bi > 1 && bj > 1 &&
+                       (points ? geometry_admissible(points, dim, d->n, p->off_h[i], bi, p->off_h[j], bj, d->admis)
+                               : std::abs(i - j) > (int)d->admis);
       if (adm) p->lslot_h[i * nb + j] = p->nlr++;
       else { p->dslot_h[i * nb + j] = p->ndense++; if (i != j) p->dense_offdiag = true; }
     }
@@ -700,6 +737,9 @@ int frank_blr_create(const frank_blr_desc* d, frank_blr** out) {
   *out = p;
   return FRANK_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int frank_blr_destroy(frank_blr* p) {
   if (!p) return FRANK_OK;
@@ -916,9 +956,13 @@ int frank_blr_get_pivots(const frank_blr* p, int i, int* ipiv) {
 int frank_blr_set_lra(frank_blr* p, const char* name, double core_scale) {
   if (!p || !name) return fail(FRANK_ERR_INVALID, "null argument");
   const std::string n(name);
-  if (n == "rounded_addition") { p->core_method = CORE_SVD; p->gram = false; }
-  else if (n == "rounded_addition_rrqr") { p->core_method = CORE_RRQR; p->gram = false; }
-  else if (n == "rounded_addition_rrqr_gram") { p->core_method = CORE_RRQR; p->gram = true; }
+  // addition.cpp:191-203: "rounded_addition" selects it for every plan; any
+  // other value selects fast_rounded_addition, which falls back to
+  // rounded_addition on tolerance plans (addition.cpp:138-143)
+  if (n == "rounded_addition") { p->core_method = CORE_SVD; p->core_fixed = CORE_SVD; p->gram = false; }
+  else if (n == "fast_rounded_addition") { p->core_method = CORE_SVD; p->core_fixed = CORE_FAST; p->gram = false; }
+  else if (n == "rounded_addition_rrqr") { p->core_method = CORE_RRQR; p->core_fixed = CORE_SVD; p->gram = false; }
+  else if (n == "rounded_addition_rrqr_gram") { p->core_method = CORE_RRQR; p->core_fixed = CORE_SVD; p->gram = true; }
   else return fail(FRANK_ERR_UNSUPPORTED, "unknown FRANK_LRA value: " + n);
   p->core_scale = core_scale > 0.0 ? core_scale : 0.1;
   if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }

@@ -109,6 +109,21 @@ FRANK_HD double rounded_addition_flops(double m, double n, double bi, double kc,
   return f;
 }
 
+// Algorithmic FLOPs of one fast rounded addition (addition.cpp:133-189) as
+// the reference issues it: projections Zu = U_C^T U_B, Zv, the residual bases,
+// their QR / RQ with explicit factors, the (kc+p) x (kc+q) core, its SVD and
+// the new bases [U_C | Q_u] U_m, V_m [V_C; Q_v].
+FRANK_HD double fast_rounded_addition_flops(double m, double n, double bi, double kc, double p, double q, double r) {
+  double f = 2.0 * p * p * bi + 2.0 * bi * q * q + 2.0 * p * bi * q;   // core of the product
+  f += 4.0 * m * kc * p + 4.0 * n * kc * q;                               // Zu, Yu; Zv, Yv
+  f += 4.0 * m * p * p - 4.0 / 3.0 * p * p * p;                           // geqrf + orgqr of Yu
+  f += 4.0 * n * q * q - 4.0 / 3.0 * q * q * q;                           // gerqf + orgrq of Yv^T
+  const double s = fmax(kc + p, kc + q);
+  f += 4.0 * s * s * s + 22.0 * s * s * s;                                // core M, gesvd
+  f += 2.0 * m * (kc + p) * r + 2.0 * n * (kc + q) * r;                   // new U, V
+  return f;
+}
+
 // ---------------------------------------------------------------------------
 // Reset the working copy from A_H (FP64) -- only the used parts are copied.
 // One CTA per block.
@@ -884,7 +899,85 @@ constexpr int SPLIT_MAX = 128;    // band-1 tasks eligible for the split (scratc
 constexpr int RECOMP_SMEM_BYTES = 227 * 1024 - 512;     // dynamic shared memory (all but the static part)
 constexpr int RECOMP_GSM = 2 * 16 * 64;                 // cta_gemm tiles (doubles)
 constexpr int RECOMP_REGION = RECOMP_SMEM_BYTES / 8 - RECOMP_GSM;  // doubles for panels / core
-enum CoreMethod { CORE_RRQR = 0, CORE_SVD = 1 };
+// Core of the recompression: RRQR (truncated pivoted QR + RQ of the core),
+// SVD (one-sided Jacobi, find_svd_truncation_rank or the fixed rank), FAST
+// (fast_rounded_addition, addition.cpp:133-189: fixed-rank targets with
+// orthonormal bases; the update's bases are projected out of the target's and
+// only the remainders are QR-factored; SVD core as above).
+enum CoreMethod { CORE_RRQR = 0, CORE_SVD = 1, CORE_FAST = 2 };
+
+// SVD of the recompression core Mm (mu x mv, ld mu; M0 holds a copy) by
+// one-sided Jacobi, in place.  Rank: the fixed rank of the plan, else
+// find_svd_truncation_rank (misc.cpp:133-146, quirk included) at ws.eps;
+// capped at kcap (counted as a rank overflow).  On return sig[ord[c]] is the
+// c-th largest singular value, Xo (bc x r, ld bc) = [U_m(:, :r); 0] and Yo
+// (bk x r, ld bk) = [V_m(:, :r); 0].  Returns r (all threads).
+template <typename T, int NT>
+FRANK_D int svd_core(int mu, int mv, double* Mm, const double* M0, const FactorWs<T>& ws, int kcap, double* sig,
+                     int* ord, double* Xo, int bc, double* Yo, int bk, double* gsm, int* flag, int* s_rank) {
+  const int sweeps = cta_jacobi_columns(mu, mv, Mm, mu, 60, flag);
+  if (sweeps < 0 && threadIdx.x == 0) atomicAdd(ws.err + ERR_JACOBI, 1);
+  for (int c = threadIdx.x >> 5; c < mv; c += blockDim.x >> 5) {
+    double sacc = 0.0;
+    for (int rr = threadIdx.x & 31; rr < mu; rr += 32) sacc += Mm[rr + (int64_t)c * mu] * Mm[rr + (int64_t)c * mu];
+    sacc = warp_sum(sacc);
+    if ((threadIdx.x & 31) == 0) sig[c] = sqrt(sacc);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < mv; c += blockDim.x) {
+    const double v = sig[c];
+    int pos = 0;
+    for (int d = 0; d < mv; ++d) {
+      const double w = sig[d];
+      pos += (w > v) || (w == v && d < c);
+    }
+    ord[pos] = c;
+  }
+  __syncthreads();
+  const int nsv = min(mu, mv);
+  if (threadIdx.x == 0) {
+    int rr;
+    if (ws.fixed_rank > 0) {
+      rr = min(ws.fixed_rank, nsv);
+    } else {
+      double fro = 0.0;
+      for (int j = 0; j < nsv; ++j) { const double v = sig[ord[j]]; fro += v * v; }
+      const double thr = ws.eps * sqrt(fro);
+      rr = 0;
+      double err;
+      do {
+        ++rr;
+        err = 0.0;
+        if (rr < nsv) {
+          const double v = sig[ord[rr]];
+          for (int j = rr; j < nsv; ++j) err += v * v;
+        }
+      } while (rr < nsv && sqrt(err) > thr);
+    }
+    if (rr > kcap) { atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1); rr = kcap; }
+    atomicMax(ws.err + ERR_MAX_RANK, rr);
+    atomicAdd(ws.err + ERR_RECOMP, 1);
+    *s_rank = rr;
+  }
+  __syncthreads();
+  const int r = *s_rank;
+  for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+    const int rr = e % bc, c = e / bc;
+    const int src = ord[c];
+    const double sv_ = sig[src];
+    Xo[e] = (rr < mu && sv_ > 0.0) ? Mm[rr + (int64_t)src * mu] / sv_ : 0.0;
+  }
+  __syncthreads();
+  // Yo (bk x r): rows < mv = M0^T Um / sigma
+  cta_gemm<double, NT>(mv, r, mu, 1.0, M0, mu, true, Xo, bc, false, 0.0, Yo, bk, gsm);
+  for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+    const int rr = e % bk, c = e / bk;
+    const double sv_ = sig[ord[c]];
+    Yo[e] = (rr < mv && sv_ > 0.0) ? Yo[e] / sv_ : 0.0;
+  }
+  __syncthreads();
+  return r;
+}
 
 struct RecompLayout {
   int64_t ash, bsh, tm, rc, rv, mtmp, mglob, m0, xo, yo, tfu, tfv, w, tau_u, tau_v, tau_c, tau2, cn, pn, jp, ji, total;
@@ -968,7 +1061,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     const int ic = i + 1 + a_, k = i + 1 + c_;
     if (!A.is_lr(ic, k)) continue;
     if (only_dense_operands && A.is_lr(ic, i) && A.is_lr(i, k)) continue;
-    const bool split_t = tsk < nspl && A.is_lr(ic, i) && A.is_lr(i, k) &&
+    const bool split_t = tsk < nspl && core_method != CORE_FAST && A.is_lr(ic, i) && A.is_lr(i, k) &&
                          max(A.rank[ic * A.nb + i], A.rank[i * A.nb + k]) > SPLIT_P;
     if ((side >= 0) != split_t) continue;
     set_base(side >= 0 ? split_base + (int64_t)tsk * ws.rscratch_stride : cta_base);
@@ -1011,6 +1104,84 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     if (do_u) form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
     SUB_MARK(10);
     PHASE_MARK(cls, 0);
+    // fast rounded addition (addition.cpp:133-189) for fixed-rank targets
+    // whose stacked bases fit the block (kc + p <= bc, kc + q <= bk); the
+    // target's U_C, V_C have orthonormal columns (rsvd construction or an
+    // earlier SVD-core recompression)
+    const bool fast = core_method == CORE_FAST && ws.fixed_rank > 0 && side < 0 && kc > 0 && o.p > 0 && o.q > 0 &&
+                      !o.left_dense && !o.right_dense && su <= bc && sv <= bk;
+    if (fast) {
+      const int mu = su, mv = sv;   // kc + p, kc + q
+      // Zu = U_C^T U_B into Rc(0:kc, kc:su), Yu = U_B - U_C Zu in place
+      cta_gemm<double, RECOMP_THREADS>(kc, o.p, bc, 1.0, Ash, bc, true, Ash + (int64_t)kc * bc, bc, false, 0.0,
+                                       Rc + (int64_t)kc * mu, mu, gsm);
+      cta_gemm<double, RECOMP_THREADS>(bc, o.p, kc, -1.0, Ash, bc, false, Rc + (int64_t)kc * mu, mu, false, 1.0,
+                                       Ash + (int64_t)kc * bc, bc, gsm);
+      // Zv = V_C^T V_B (ZvT of the reference transposed), Yv = V_B - V_C Zv
+      cta_gemm<double, RECOMP_THREADS>(kc, o.q, bk, 1.0, Bsh, bk, true, Bsh + (int64_t)kc * bk, bk, false, 0.0,
+                                       Rv + (int64_t)kc * mv, mv, gsm);
+      cta_gemm<double, RECOMP_THREADS>(bk, o.q, kc, -1.0, Bsh, bk, false, Rv + (int64_t)kc * mv, mv, false, 1.0,
+                                       Bsh + (int64_t)kc * bk, bk, gsm);
+      PHASE_MARK(cls, 1);
+      cta_qr_blocked<RECOMP_THREADS>(bc, o.p, Ash + (int64_t)kc * bc, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
+      cta_qr_blocked<RECOMP_THREADS>(bk, o.q, Bsh + (int64_t)kc * bk, bk, tau_v, Tfv, Wq, smP, smT, gsm, red);
+      PHASE_MARK(cls, 2);
+      // Rc = [I Zu; 0 Ru] (mu x su), Rv = [I Zv; 0 Rv'] (mv x sv)
+      for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
+        const int r = e % mu, c = e / mu;
+        if (c < kc) Rc[e] = (r == c) ? 1.0 : 0.0;
+        else if (r >= kc) Rc[e] = (r - kc <= c - kc) ? Ash[(r - kc) + (int64_t)c * bc] : 0.0;
+      }
+      for (int64_t e = threadIdx.x; e < (int64_t)mv * sv; e += blockDim.x) {
+        const int r = e % mv, c = e / mv;
+        if (c < kc) Rv[e] = (r == c) ? 1.0 : 0.0;
+        else if (r >= kc) Rv[e] = (r - kc <= c - kc) ? Bsh[(r - kc) + (int64_t)c * bk] : 0.0;
+      }
+      __syncthreads();
+      // core M (mu x mv) = Rc blockdiag(S_C, T) Rv^T
+      cta_gemm<double, RECOMP_THREADS>(mu, kc, kc, 1.0, Rc, mu, false, Sc, A.kcap, false, 0.0, Mtmp, mu, gsm);
+      cta_gemm<double, RECOMP_THREADS>(mu, o.q, o.p, 1.0, Rc + (int64_t)kc * mu, mu, false, Tm, o.p, false, 0.0,
+                                       Mtmp + (int64_t)kc * mu, mu, gsm);
+      const bool in_smem = (int64_t)mu * mv <= RECOMP_REGION;
+      double* Mm = in_smem ? region : Mg;
+      cta_gemm<double, RECOMP_THREADS>(mu, mv, sv, 1.0, Mtmp, mu, false, Rv, mv, true, 0.0, Mm, mu, gsm);
+      PHASE_MARK(cls, 3);
+      for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) M0[e] = Mm[e];
+      __syncthreads();
+      const int r = svd_core<T, RECOMP_THREADS>(mu, mv, Mm, M0, ws, A.kcap, cnorm, jpvt, Xo, bc, Yo, bk, gsm, &flag, &s_rank);
+      for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
+        const int rr = e % r, c = e / r;
+        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? cnorm[jpvt[c]] : 0.0);
+      }
+      PHASE_MARK(cls, 4);
+      if (threadIdx.x == 0)
+        atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)fast_rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r));
+      // U = [U_C | Q_u] Xo = Q_u [Xo(kc:mu); 0] + U_C Xo(0:kc), through Tm
+      // (bc x r); U_C is read from its FP64 copy in Ash, so Uc is written last
+      for (int side2 = 0; side2 < 2; ++side2) {
+        const int bb = side2 ? bk : bc, pp = side2 ? o.q : o.p;
+        double* X = side2 ? Yo : Xo;
+        double* Bs = side2 ? Bsh : Ash;
+        T* out = side2 ? Vc : Uc;
+        for (int64_t e = threadIdx.x; e < (int64_t)bb * r; e += blockDim.x) {
+          const int rr = e % bb, c = e / bb;
+          Tm[e] = rr < pp ? X[kc + rr + (int64_t)c * bb] : 0.0;
+        }
+        __syncthreads();
+        cta_apply_q_blocked<RECOMP_THREADS>(bb, pp, Bs + (int64_t)kc * bb, bb, side2 ? Tfv : Tfu, r, Tm, (int64_t)bb,
+                                            Wq, smP, smT, gsm, pp);
+        cta_gemm<double, RECOMP_THREADS>(bb, r, kc, 1.0, Bs, bb, false, X, bb, false, 1.0, Tm, bb, gsm);
+        for (int64_t e = threadIdx.x; e < (int64_t)bb * r; e += blockDim.x) {
+          const int rr = e % bb, c = e / bb;
+          out[rr + (int64_t)c * ld] = T(Tm[e]);
+        }
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) A.rank[blk] = r;
+      __syncthreads();
+      PHASE_MARK(cls, 5);
+      continue;
+    }
     if (do_u) cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
     PHASE_MARK(cls, 1);
     // the V side of a split target works in Mtmp (free until the core), so
@@ -1125,71 +1296,10 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       // SVD core: keep a copy for the V side, Jacobi in place
       for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) M0[e] = Mm[e];
       __syncthreads();
-      const int sweeps = cta_jacobi_columns(mu, mv, Mm, mu, 60, &flag);
-      if (sweeps < 0 && threadIdx.x == 0) atomicAdd(ws.err + ERR_JACOBI, 1);
-      double* sig = cnorm;
-      int* ord = jpvt;
-      for (int c = threadIdx.x >> 5; c < mv; c += blockDim.x >> 5) {
-        double sacc = 0.0;
-        for (int rr = threadIdx.x & 31; rr < mu; rr += 32) sacc += Mm[rr + (int64_t)c * mu] * Mm[rr + (int64_t)c * mu];
-        sacc = warp_sum(sacc);
-        if ((threadIdx.x & 31) == 0) sig[c] = sqrt(sacc);
-      }
-      __syncthreads();
-      for (int c = threadIdx.x; c < mv; c += blockDim.x) {
-        const double v = sig[c];
-        int pos = 0;
-        for (int d = 0; d < mv; ++d) {
-          const double w = sig[d];
-          pos += (w > v) || (w == v && d < c);
-        }
-        ord[pos] = c;
-      }
-      __syncthreads();
-      const int nsv = min(mu, mv);
-      if (threadIdx.x == 0) {
-        int rr;
-        if (ws.fixed_rank > 0) {
-          rr = min(ws.fixed_rank, nsv);
-        } else {
-          double fro = 0.0;
-          for (int j = 0; j < nsv; ++j) { const double v = sig[ord[j]]; fro += v * v; }
-          const double thr = ws.eps * sqrt(fro);
-          rr = 0;
-          double err;
-          do {
-            ++rr;
-            err = 0.0;
-            if (rr < nsv) {
-              const double v = sig[ord[rr]];
-              for (int j = rr; j < nsv; ++j) err += v * v;
-            }
-          } while (rr < nsv && sqrt(err) > thr);
-        }
-        if (rr > A.kcap) { atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1); rr = A.kcap; }
-        atomicMax(ws.err + ERR_MAX_RANK, rr);
-        atomicAdd(ws.err + ERR_RECOMP, 1);
-        s_rank = rr;
-      }
-      __syncthreads();
-      r = s_rank;
-      for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
-        const int rr = e % bc, c = e / bc;
-        const int src = ord[c];
-        const double sv_ = sig[src];
-        Xo[e] = (rr < mu && sv_ > 0.0) ? Mm[rr + (int64_t)src * mu] / sv_ : 0.0;
-      }
-      __syncthreads();
-      // Yo (bk x r): rows < mv = M0^T Um / sigma
-      cta_gemm<double, RECOMP_THREADS>(mv, r, mu, 1.0, M0, mu, true, Xo, bc, false, 0.0, Yo, bk, gsm);
-      for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
-        const int rr = e % bk, c = e / bk;
-        const double sv_ = sig[ord[c]];
-        Yo[e] = (rr < mv && sv_ > 0.0) ? Yo[e] / sv_ : 0.0;
-      }
+      r = svd_core<T, RECOMP_THREADS>(mu, mv, Mm, M0, ws, A.kcap, cnorm, jpvt, Xo, bc, Yo, bk, gsm, &flag, &s_rank);
       for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
         const int rr = e % r, c = e / r;
-        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? sig[ord[c]] : 0.0);
+        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? cnorm[jpvt[c]] : 0.0);
       }
       __syncthreads();
     }

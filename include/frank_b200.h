@@ -83,6 +83,14 @@ int frank_device_info(char* name, int name_len, int* sm_count, int* cc_major, in
  * Hierarchical(n_row_blocks, n_col_blocks) (classes/hierarchical.cpp:46-47). */
 int frank_blr_create(const frank_blr_desc* desc, frank_blr** out);
 
+/* Create a plan whose admissibility is geometry-based: off-diagonal block
+ * (i, j) is low rank iff admis^2 diam^2 < dist^2 for the bounding boxes of
+ * its row and column points padded by 0.5 (AdmisType::GeometryBased,
+ * classes/initialization_helpers/matrix_initializer.cpp:51-91).  points:
+ * dim x n, axis-major (params[d][i], functions.h:34-38), host FP64; desc->admis
+ * is the admissibility constant. */
+int frank_blr_create_geometric(const frank_blr_desc* desc, const double* points, int dim, frank_blr** out);
+
 /* Free all device memory of the plan. */
 int frank_blr_destroy(frank_blr* plan);
 
@@ -134,15 +142,23 @@ int frank_blr_get_pivots(const frank_blr* plan, int i, int* ipiv);
  * setGlobalValue("FRANK_LRA", name) (util/global_key_value.cpp:10-22, read at
  * operations/arithmetic/addition.cpp:194-201):
  *   "rounded_addition"       core SVD (one-sided Jacobi, FP64) truncated by
- *                            find_svd_truncation_rank -- the reference algorithm;
- *   "rounded_addition_rrqr"  (default) the reference's fixed-accuracy compressor
+ *                            find_svd_truncation_rank -- the reference algorithm
+ *                            selected by FRANK_LRA=rounded_addition;
+ *   "fast_rounded_addition"  (default of fixed-rank plans, as in the reference
+ *                            with FRANK_LRA unset, addition.cpp:133-189) the
+ *                            update's bases projected out of the target's
+ *                            orthonormal ones, QR of the remainders only, core
+ *                            SVD; on tolerance plans it falls back to
+ *                            "rounded_addition" like the reference;
+ *   "rounded_addition_rrqr"  (default of tolerance plans) the reference's fixed-accuracy compressor
  *                            truncated_geqp3 + rq applied to the same core, with
  *                            tolerance core_scale * eps (core_scale <= 0: 0.1);
  *   "rounded_addition_rrqr_gram"  mixed plans only: the same RRQR core, with the
  *                            stacked bases orthogonalised through their FP64
  *                            Gram matrices (pivoted Cholesky) instead of a
  *                            Householder QR along the block rows.
- * Fixed-rank plans always use the core SVD. */
+ * Fixed-rank plans use the core SVD under every value but
+ * "fast_rounded_addition" and the default. */
 int frank_blr_set_lra(frank_blr* plan, const char* name, double core_scale);
 
 /* Right-looking block LU in place.  Replaces getrf(Hierarchical&)

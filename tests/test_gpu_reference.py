@@ -1,0 +1,196 @@
+"""GPU parity against the reference's own outputs.
+
+tests/golden/reference_blr.json and reference_vectors.npz hold what FRANK
+itself (its C++ sources compiled unmodified into oracle/_ref and run through
+its public API; tests/golden/make_ref_golden.py) produced on its BLR test
+grids, on the fixed-rank Laplace-1D N=2048 workload and on the leading 8 x 8
+blocks (N=4096) of the headline Laplace-3D point set.  The CUDA path runs the
+same cases through the C ABI, on A_H built by the oracle (whose per-block
+ranks equal the reference's on every grid case, test_oracle_vs_reference.py),
+with the same LowRank addition the reference ran:
+
+* FRANK_LRA=rounded_addition (the core SVD truncated by
+  find_svd_truncation_rank, quirk included) on the fixed-accuracy grid,
+  position- and geometry-based admissibility;
+* the default fast_rounded_addition and rounded_addition on the fixed-rank
+  grid and the N=2048 workload.
+
+Stated tolerances: per-block ranks of the factor within RANK_TOL of the
+reference's (a singular value at the truncation threshold may fall either
+side under roundoff); solve errors <= eps (the reference's own criterion) and
+within ERR_FACTOR of the reference's plus a roundoff floor; solutions within
+a relative 1e-9 (fixed rank) or 10 eps (tolerance) of the reference's."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle.frank_oracle as fo
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF = json.load(open(os.path.join(GOLD, "reference_blr.json")))
+VEC = np.load(os.path.join(GOLD, "reference_vectors.npz"))
+RANK_TOL = 1
+ERR_FACTOR, ERR_FLOOR = 5.0, 1e-13
+
+
+def _plan(A, n, nb, *, admis, admis_type, x, **kw):
+    from frank_b200 import BLRMatrix
+    M = BLRMatrix(n, nb, admis=admis, admis_type=admis_type, points=x, **kw)
+    for i in range(nb):
+        for j in range(nb):
+            blk = A[i, j]
+            if isinstance(blk, np.ndarray):
+                M.set_dense(i, j, blk)
+            else:
+                M.set_lowrank(i, j, blk.U, blk.S, blk.V)
+    return M
+
+
+def _gpu_ranks(M, n_lr_only=True):
+    nb = M.nb
+    return [M.rank(i, j, 1) if M.is_lowrank(i, j) else -1 for i in range(nb) for j in range(nb)]
+
+
+def _case_id(c):
+    tag = ("e%g" % c["eps"]) if "eps" in c else ("k%d" % c["rank"])
+    return "%s-n%d-%s-a%g-%s" % (c["lra"], c["n"], tag, c["admis"], c["admis_type"])
+
+
+CASES = REF["cases"]
+
+
+@pytest.mark.parametrize("c", CASES, ids=[_case_id(c) for c in CASES])
+def test_blr_grid_matches_reference(gpu_lib, c):
+    n, nleaf = c["n"], c["nleaf"]
+    nb = n // nleaf
+    x = np.array([fo.get_sorted_random_vector(n)])
+    at = fo.GEOMETRY_BASED if c["admis_type"] == "geometry" else fo.POSITION_BASED
+    fixed = "rank" in c
+    kw = dict(rank=c["rank"]) if fixed else dict(eps=c["eps"])
+    A = fo.build_hierarchical(fo.laplacend, x, n, nleaf, nb, admis=c["admis"], admis_type=at, **kw)
+    M = _plan(A, n, nb, admis=c["admis"], admis_type=c["admis_type"], x=x,
+              **(dict(fixed_rank=c["rank"]) if fixed else dict(eps=c["eps"])))
+    M.set_lra(c["lra"])
+    # the plan's block types are the reference's (its A_H ranks, -1 = dense)
+    assert [M.rank(i, j, 0) if M.is_lowrank(i, j) else -1 for i in range(nb) for j in range(nb)] == c["ranks_h"]
+    xv = fo.random_uniform(n, 1)
+    b = fo.matvec(A, xv)
+    M.getrf()
+    for i in range(nb):                      # the reference drops pivots: none may occur here
+        assert np.array_equal(M.pivots(i), np.arange(1, M.block_size(i) + 1))
+    got = _gpu_ranks(M)
+    ref = [max(l, u) for l, u in zip(c["ranks_l"], c["ranks_u"])]
+    assert all(abs(g - r) <= RANK_TOL for g, r in zip(got, ref)), (got, ref)
+    err = fo.l2_error(xv, M.solve(b))
+    if not fixed:
+        assert err <= c["eps"]                                    # blr_fixed_acc_test.cpp:82
+    assert err <= ERR_FACTOR * c["solve_error"] + ERR_FLOOR, (err, c["solve_error"])
+    M.close()
+
+
+@pytest.mark.parametrize("lra", ["fast", "rounded_addition"])
+def test_fixed_rank_2048_matches_reference(gpu_lib, lra):
+    """Laplace-1D N=2048, 8 x 8 blocks of 256, rank 16, with the LowRank
+    addition the reference ran (its default fast_rounded_addition, or
+    rounded_addition): solution and the singular values of every low-rank
+    factor block against the reference's."""
+    tag = "cfg1_" + lra
+    n, nb, rank = 2048, 8, 16
+    x = np.array([fo.get_sorted_random_vector(n)])
+    A = fo.build_hierarchical(fo.laplacend, x, n, 256, nb, rank=rank)
+    M = _plan(A, n, nb, admis=0.0, admis_type="position", x=x, fixed_rank=rank)
+    M.set_lra("fast_rounded_addition" if lra == "fast" else lra)
+    xv = fo.random_uniform(n, 1)
+    b = fo.matvec(A, xv)
+    M.getrf()
+    xs = M.solve(b)[:, 0]
+    xr = VEC[tag + "/x"]
+    assert np.linalg.norm(xs - xr) <= 1e-9 * np.linalg.norm(xr)
+    for i in range(nb):
+        for j in range(nb):
+            side = "L" if i > j else "U"
+            key = "%s/sv/%s/%d/%d" % (tag, side, i, j)
+            if i != j:
+                U, S, V = M.block(i, j, which=1)
+                sv = np.linalg.svd(U @ S @ V, compute_uv=False)[: len(VEC[key])]
+                np.testing.assert_allclose(sv, VEC[key], rtol=1e-8, atol=1e-12 * VEC[key][0])
+            else:
+                ud = np.diag(M.block(i, i, which=1))
+                np.testing.assert_allclose(ud, VEC["%s/udiag/%d" % (tag, i)], rtol=1e-10)
+    M.close()
+
+
+@pytest.fixture(scope="module")
+def headline4096():
+    """The leading 8 x 8 blocks of 512 (N=4096) of the headline Laplace-3D
+    point set (std::mt19937_64 seed 2, Morton ordered), A_H at eps 1e-8 by
+    the oracle, 4 right-hand sides (std::mt19937_64 seed 3)."""
+    from bench import make_points, make_rhs
+    n, nb = 4096, 8
+    x = make_points(32768, 3, 2, 10)[:, :n].copy()
+    b = make_rhs(n, 4, 3)
+    np.testing.assert_allclose([x.sum(), (x * x).sum()], VEC["headline4096/points_checksum"], rtol=1e-14)
+    np.testing.assert_allclose([b.sum(), (b * b).sum()], VEC["headline4096/rhs_checksum"], rtol=1e-12)
+    A = fo.build_hierarchical(fo.laplacend, x, n, 512, nb, eps=1e-8)
+    Ad = fo.to_dense(A)
+    xd = np.linalg.solve(Ad, b)
+    return dict(x=x, b=b, A=A, Ad=Ad, xd=xd, n=n, nb=nb)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_headline4096_fp64_matches_reference(gpu_lib, headline4096):
+    """FP64 plan with the reference's rounded_addition at eps 1e-8: ranks,
+    block singular values, solution vs the reference's and vs dense LAPACK."""
+    h = headline4096
+    meta = REF["vectors_meta"]["headline4096"]
+    M = _plan(h["A"], h["n"], h["nb"], admis=0.0, admis_type="position", x=h["x"], eps=1e-8)
+    M.set_lra("rounded_addition")
+    M.getrf()
+    got = _gpu_ranks(M)
+    ref = [max(l, u) for l, u in zip(meta["ranks_l"], meta["ranks_u"])]
+    assert all(abs(g - r) <= RANK_TOL for g, r in zip(got, ref)), (got, ref)
+    xs = M.solve(h["b"])
+    xr = VEC["headline4096/x"].reshape(4, h["n"]).T
+    # the reference's own error against the dense solve, and ours
+    ref_err, gpu_err = _rel(xr, h["xd"]), _rel(xs, h["xd"])
+    assert gpu_err <= ERR_FACTOR * ref_err + 1e-13, (gpu_err, ref_err)
+    assert _rel(xs, xr) <= 10 * 1e-8
+    res = np.linalg.norm(h["b"] - fo.matvec(h["A"], xs)) / np.linalg.norm(h["b"])
+    assert res <= ERR_FACTOR * meta["residual"] + 1e-15, (res, meta["residual"])
+    # singular values of the low-rank factor blocks, down to eps of the largest
+    for i in range(h["nb"]):
+        for j in range(h["nb"]):
+            if i == j:
+                continue
+            key = "headline4096/sv/%s/%d/%d" % ("L" if i > j else "U", i, j)
+            U, S, V = M.block(i, j, which=1)
+            sv = np.linalg.svd(U @ S @ V, compute_uv=False)
+            rv = VEC[key]
+            k = int(np.sum(rv > 1e-6 * rv[0]))
+            np.testing.assert_allclose(sv[:k], rv[:k], rtol=1e-6)
+    M.close()
+
+
+@pytest.mark.parametrize("lra", ["rounded_addition", "rounded_addition_rrqr"])
+def test_headline4096_mixed_refined_matches_reference(gpu_lib, headline4096, lra):
+    """Mixed plan (FP32 factor at 3e-3, the bench's setting) + FP64 refinement
+    to 1e-10: the refined solution against the reference's and the dense one."""
+    from frank_b200 import BLRMatrix
+    h = headline4096
+    M = _plan(h["A"], h["n"], h["nb"], admis=0.0, admis_type="position", x=h["x"], eps=3e-3, precision="mixed")
+    M.set_lra(lra)
+    M.getrf()
+    xs, it, res = M.refine(h["b"], tol=1e-10, maxit=30)
+    assert res <= 1e-10
+    xr = VEC["headline4096/x"].reshape(4, h["n"]).T
+    ref_err = _rel(xr, h["xd"])
+    # refinement solves A_H x = b to 1e-10; A_H differs from A by <= eps = 1e-8
+    assert _rel(xs, h["xd"]) <= max(ERR_FACTOR * ref_err, 1e-9)
+    assert _rel(xs, xr) <= 10 * 1e-8
+    M.close()
