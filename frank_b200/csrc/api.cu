@@ -110,6 +110,19 @@ struct frank_blr {
   bool timed = false;  // timing events recorded in the captured graph (opt-in:
                        // event-record nodes serialise the graph's branches)
   bool want_timing = false;
+  // captured solves (graph of cast / diagonal / scatter launches), keyed by
+  // buffer, leading dimension, RHS count and direction
+  struct SolveGraph {
+    cudaGraphExec_t exec = nullptr;
+    const void* ptr = nullptr;
+    int64_t ld = 0;
+    int nrhs = 0;
+    bool transpose = false;
+    int64_t kernels = 0;
+  };
+  std::vector<SolveGraph> solve_graphs;
+  cudaStream_t cap_stream = nullptr;   // private stream the solves are captured on
+  int solve_chunk = 8;                 // RHS per solve pass (bounded by the scatter's shared memory)
   // lookahead: second capture stream and its dependency events
   cudaStream_t aux = nullptr;
   cudaEvent_t fork = nullptr;
@@ -383,11 +396,11 @@ int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cud
   const int nb = p->nb;
   const int gd = (p->bmax + SOLVE_ROWS - 1) / SOLVE_ROWS;
   const size_t shd = ((size_t)p->bmax * nrhs + (size_t)(SOLVE_THREADS / SOLVE_ROWS) * SOLVE_ROWS * 8) * sizeof(double);
-  const size_t shs = ((size_t)p->bmax * nrhs + 2 * (size_t)p->kcap * nrhs) * sizeof(double);
-  p->solve_launches += 4 * nb;
+  const size_t shs = solve_scatter_cl_smem(p->bmax, p->kcap, nrhs);
   auto step = [&](int i, int dmode, int smode, int ntarget) {
     k_solve_diag<T><<<gd, SOLVE_THREADS, shd, s>>>(W, ws, i, z, ldz, nrhs, dmode, ybuf);
-    k_solve_scatter<T><<<ntarget + 1, SOLVE_THREADS, shs, s>>>(W, i, z, ldz, nrhs, smode, ybuf, ntarget);
+    k_solve_scatter_cl<T><<<std::max(ntarget, 1) * SC_CLUSTER, SOLVE_THREADS, shs, s>>>(W, i, z, ldz, nrhs, smode,
+                                                                                       ybuf, ntarget);
   };
   if (!transpose) {
     for (int i = 0; i < nb; ++i) step(i, 0, 0, nb - i - 1);
@@ -402,18 +415,18 @@ int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cud
 
 int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 4096); }
 
-// d_b (double, n x nrhs) -> solve in T -> back into d_b.
-int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s) {
-  if (!p->factored) return fail(FRANK_ERR_STATE, "solve before getrf");
-  for (int c0 = 0; c0 < nrhs; c0 += 8) {
-    const int nr = std::min(8, nrhs - c0);
+// Enqueue the launches of one solve of d_b (double, n x nrhs, in place): the
+// FP64 plan solves in place, the mixed plan casts to its FP32 vector, solves
+// and casts back.
+int enqueue_solve_all(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s) {
+  for (int c0 = 0; c0 < nrhs; c0 += p->solve_chunk) {
+    const int nr = std::min(p->solve_chunk, nrhs - c0);
     double* b = d_b + c0 * ldb;
     if (p->precision == FRANK_PREC_FP64) {
       int rc = enqueue_solve<double>(p, b, ldb, nr, transpose, s);
       if (rc) return rc;
     } else {
       float* z = static_cast<float*>(p->z);
-      p->solve_launches += 2;
       k_cast_copy<float, double><<<grid_for(p->n * nr), 256, 0, s>>>(b, ldb, z, p->n, p->n, nr);
       int rc = enqueue_solve<float>(p, z, p->n, nr, transpose, s);
       if (rc) return rc;
@@ -424,12 +437,50 @@ int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool tra
   return FRANK_OK;
 }
 
+void drop_solve_graphs(frank_blr* p) {
+  for (auto& g : p->solve_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  p->solve_graphs.clear();
+}
+
+// d_b (double, n x nrhs) -> solve in T -> back into d_b.  The 2 nb launches
+// per pass are captured once per (buffer, ld, nrhs, direction) on the plan's
+// private capture stream and replayed as one graph launch on `s`.
+int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s) {
+  if (!p->factored) return fail(FRANK_ERR_STATE, "solve before getrf");
+  frank_blr::SolveGraph* hit = nullptr;
+  for (auto& g : p->solve_graphs)
+    if (g.ptr == d_b && g.ld == ldb && g.nrhs == nrhs && g.transpose == transpose) hit = &g;
+  if (!hit) {
+    if (!p->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+    if (p->solve_graphs.size() >= 4) drop_solve_graphs(p);
+    CUDA_TRY(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_solve_all(p, d_b, ldb, nrhs, transpose, p->cap_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
+    if (rc != FRANK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("solve capture: ") + cudaGetErrorString(e));
+    frank_blr::SolveGraph sg;
+    size_t nodes = 0;
+    cudaGraphGetNodes(g, nullptr, &nodes);
+    e = cudaGraphInstantiate(&sg.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("solve graph: ") + cudaGetErrorString(e));
+    sg.ptr = d_b; sg.ld = ldb; sg.nrhs = nrhs; sg.transpose = transpose; sg.kernels = (int64_t)nodes;
+    p->solve_graphs.push_back(sg);
+    hit = &p->solve_graphs.back();
+  }
+  p->solve_launches += hit->kernels;
+  CUDA_TRY(cudaGraphLaunch(hit->exec, s));
+  return FRANK_OK;
+}
+
 int matvec_device_impl(frank_blr* p, const double* x, int64_t ldx, double* y, int64_t ldy, int nrhs,
                        const double* bres, int64_t ldb, cudaStream_t s, bool transpose = false) {
   BlrView<double> H = h_view(p);
   for (int c0 = 0; c0 < nrhs; c0 += 8) {
     const int nr = std::min(8, nrhs - c0);
-    const size_t shm = 2 * (size_t)p->kcap * nr * sizeof(double);
+    const size_t shm = matvec_smem(p->bmax, p->kcap, nr);
     p->solve_launches += 2;
     k_matvec_blocks<<<dim3(p->nb, p->nb), MV_THREADS, shm, s>>>(H, x + c0 * ldx, ldx, nr, p->part, transpose ? 1 : 0);
     k_matvec_reduce<<<p->nb, 256, 0, s>>>(H, p->part, nr, bres ? bres + c0 * ldb : nullptr, ldb, y + c0 * ldy, ldy);
@@ -477,11 +528,15 @@ int refine_device_impl(frank_blr* p, const double* b, int64_t ldb, double* x, in
   int rc;
   std::vector<double> bn, rn;
   if ((rc = colnorms(p, b, ldb, nrhs, bn, s))) return rc;
-  // x0 = (LU)^{-1} b
-  CUDA_TRY(cudaMemcpy2DAsync(x, ldx * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
-                             cudaMemcpyDeviceToDevice, s));
-  if ((rc = solve_device_impl(p, x, ldx, nrhs, transpose, s))) return rc;
+  // every solve acts on the plan's residual / correction buffer r, so one
+  // captured solve graph serves the whole refinement
   double* r = p->vtmp;  // n x nrhs residual / correction
+  // x0 = (LU)^{-1} b
+  CUDA_TRY(cudaMemcpy2DAsync(r, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyDeviceToDevice, s));
+  if ((rc = solve_device_impl(p, r, p->n, nrhs, transpose, s))) return rc;
+  CUDA_TRY(cudaMemcpy2DAsync(x, ldx * sizeof(double), r, p->n * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyDeviceToDevice, s));
   int it = 0;
   double res = 0.0;
   for (;;) {
@@ -518,6 +573,8 @@ void free_plan(frank_blr* p) {
   if (p->fork) cudaEventDestroy(p->fork);
   if (p->aux) cudaStreamDestroy(p->aux);
   if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
+  drop_solve_graphs(p);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   if (p->nrm_h) cudaFreeHost(p->nrm_h);
   delete p;
 }
@@ -719,13 +776,17 @@ int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_bl
     free_plan(p);
     return fail(FRANK_ERR_CUDA, "plan upload");
   }
-  // dynamic shared memory of the solve / matvec kernels (kcap * 8 RHS * 2 doubles)
-  const int shm = (int)(2 * kc * 8 * sizeof(double));
-  const int shs = (int)((bm * 8 + 2 * kc * 8) * sizeof(double));
+  // dynamic shared memory of the solve / matvec kernels (8 RHS per pass)
+  const int shm = (int)matvec_smem((int)bm, (int)kc, 8);
   const int shd = (int)((bm * 8 + (SOLVE_THREADS / SOLVE_ROWS) * SOLVE_ROWS * 8) * sizeof(double));
+  // RHS per solve pass: the most whose scatter shared memory fits a CTA
+  p->solve_chunk = 8;
+  while (p->solve_chunk > 1 && solve_scatter_cl_smem((int)bm, (int)kc, p->solve_chunk) > (size_t)SMEM_OPTIN_MAX)
+    p->solve_chunk /= 2;
+  const int shs = (int)solve_scatter_cl_smem((int)bm, (int)kc, p->solve_chunk);
   cudaFuncSetAttribute(k_matvec_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
-  cudaFuncSetAttribute(k_solve_scatter<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
-  cudaFuncSetAttribute(k_solve_scatter<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
+  cudaFuncSetAttribute(k_solve_scatter_cl<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
+  cudaFuncSetAttribute(k_solve_scatter_cl<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shs);
   cudaFuncSetAttribute(k_solve_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, shd);
   cudaFuncSetAttribute(k_solve_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, shd);
   cudaFuncSetAttribute(k_trinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRINV_SMEM_MAX);

@@ -11,6 +11,8 @@
 
 #include "common.cuh"
 
+#include <cooperative_groups.h>
+
 namespace frank {
 
 template <typename T>
@@ -1718,7 +1720,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, Fact
           if (c < nrhs) acc[c] += mv * xs[t + c * b];
       }
     }
-    for (int c = 0; c < nrhs; ++c) part[(sl * SOLVE_ROWS + rl) * 8 + c] = acc[c];
+    #pragma unroll
+    for (int c = 0; c < 8; ++c) if (c < nrhs) part[(sl * SOLVE_ROWS + rl) * 8 + c] = acc[c];
     __syncthreads();
     for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
       const int r = e % nr, c = e / nr;
@@ -1742,7 +1745,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, Fact
         for (int c = 0; c < 8; ++c)
           if (c < nrhs) acc[c] += mv * xs[t + c * b];
       }
-      for (int c = 0; c < nrhs; ++c) {
+      #pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c >= nrhs) break;
         const double sum = warp_sum(acc[c]);
         if (lane == 0) ybuf[(which == 3 ? perm[r] : r) + (int64_t)c * ld] = T(sum);
       }
@@ -1750,118 +1755,237 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, Fact
   }
 }
 
-// z_j -= Blk z_i using the solved block y_i in ybuf, for every target j of
-// the step (one CTA each); CTA number `ntarget` copies y_i into z_i.
+// z_j -= Blk y_i for every target j of step i, with the solved block y_i in
+// ybuf, then z_i = y_i:
 // mode 0: targets j > i using blocks (j, i)        [forward, L]
 // mode 1: targets j < i using blocks (j, i)        [backward, U]
 // mode 2: targets j > i using blocks (i, j)^T      [transpose forward, U^T]
 // mode 3: targets j < i using blocks (i, j)^T      [transpose backward, L^T]
+// One thread-block cluster of SC_CLUSTER CTAs per target j (grid =
+// max(ntarget, 1) clusters; the first cluster also copies y_i into z_i).  For a low-rank block U S V^T the cluster's CTAs split the
+// work three ways and exchange the pieces through distributed shared memory:
+//   A: CTA q contracts columns [q cw, (q+1) cw) of the inner basis with y_i
+//      (t1 = inner^T y, one warp per column);
+//   B: after a cluster barrier every CTA gathers all of t1, then CTA q forms
+//      rows [q cw, (q+1) cw) of t2 = S t1 (S^T t1 when transposing);
+//   C: after a second barrier every CTA gathers all of t2 and updates its
+//      row tile z_j(tile) -= outer(tile, :) t2.
+// A third barrier keeps every CTA's shared memory alive until the gathers of
+// the others are done.  A dense block is applied tile by tile in phase C.
+// Every CTA reaches the three barriers.
+constexpr int SC_CLUSTER = 8;
+constexpr int SMEM_OPTIN_MAX = 227 * 1024;   // dynamic shared memory a CTA may opt into
+
+// Rows of t2 per CTA at most (the stride of the phase-B partial sums).
+FRANK_HD int solve_cl_rows(int kcap) { return (kcap + SC_CLUSTER - 1) / SC_CLUSTER; }
+
+// Doubles of the partial-sum area: phase B (SOLVE_THREADS / 32 warps x
+// solve_cl_rows x 8) and phase C (SOLVE_THREADS / 64 splits x 64 rows x 8).
+FRANK_HD int64_t solve_cl_part(int kcap) {
+  const int64_t b = (int64_t)(SOLVE_THREADS / 32) * solve_cl_rows(kcap) * 8, c = (int64_t)(SOLVE_THREADS / 64) * 64 * 8;
+  return b > c ? b : c;
+}
+
+// dynamic shared memory: ys (bmax x nrhs), t1, t2 (kcap x nrhs each) and the
+// partial sums
+FRANK_HD size_t solve_scatter_cl_smem(int bmax, int kcap, int nrhs) {
+  return ((size_t)bmax * nrhs + 2 * (size_t)kcap * nrhs + (size_t)solve_cl_part(kcap)) * sizeof(double);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve_scatter(BlrView<T> A, int i, T* z, int64_t ldz, int nrhs,
-                                                                 int mode, const T* ybuf, int ntarget) {
-  extern __shared__ double ssm[];   // y_i (bi x nrhs), t1, t2 (kcap x nrhs each)
+__global__ void __cluster_dims__(SC_CLUSTER, 1, 1) __launch_bounds__(SOLVE_THREADS)
+    k_solve_scatter_cl(BlrView<T> A, int i, T* z, int64_t ldz, int nrhs, int mode, const T* ybuf, int ntarget) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ double csm[];
   const int ld = A.bmax;
   const int bi = A.bs(i);
   const int64_t oi = A.off[i];
-  if ((int)blockIdx.x == ntarget) {
-    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
-      const int r = e % bi, c = e / bi;
+  const int q = (int)cl.block_rank();
+  const int t = blockIdx.x / SC_CLUSTER;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double* ys = csm;
+  double* t1 = ys + (int64_t)A.bmax * nrhs;
+  double* t2 = t1 + (int64_t)A.kcap * nrhs;
+  double* part = t2 + (int64_t)A.kcap * nrhs;   // partial sums (solve_cl_part doubles)
+  const int pstride = solve_cl_rows(A.kcap);
+  // y_i -> z_i, one row tile per CTA of the first cluster
+  if (t == 0) {
+    const int tl = (bi + SC_CLUSTER - 1) / SC_CLUSTER, r0 = q * tl, r1 = min(bi, r0 + tl);
+    for (int e = threadIdx.x; e < (r1 - r0) * nrhs; e += blockDim.x) {
+      const int r = r0 + e % (r1 - r0), c = e / (r1 - r0);
       z[oi + r + (int64_t)c * ldz] = ybuf[r + (int64_t)c * ld];
     }
-    return;
   }
-  const int j = (mode == 0 || mode == 2) ? i + 1 + blockIdx.x : (int)blockIdx.x;
-  const int bj = A.bs(j);
-  const int64_t oj = A.off[j];
+  const bool active = t < ntarget;
   const bool tr = (mode >= 2);
-  const int bi_ = tr ? i : j, bj_ = tr ? j : i;  // block (bi_, bj_)
-  double* ys = ssm;
-  double* t1 = ys + (int64_t)bi * nrhs;
-  double* t2 = t1 + (int64_t)A.kcap * nrhs;
-  for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
-    const int r = e % bi, c = e / bi;
-    ys[e] = double(ybuf[r + (int64_t)c * ld]);
+  int j = 0, bj = 0, r = 0, bi_ = 0, bj_ = 0;
+  bool lr = false;
+  if (active) {
+    j = (mode == 0 || mode == 2) ? i + 1 + t : t;
+    bj = A.bs(j);
+    bi_ = tr ? i : j;
+    bj_ = tr ? j : i;
+    lr = A.is_lr(bi_, bj_);
+    r = lr ? A.rank[bi_ * A.nb + bj_] : 0;
+  }
+  const int cw = (r + SC_CLUSTER - 1) / SC_CLUSTER;   // columns of t1 / rows of t2 per CTA
+  const int c0 = min(r, q * cw), c1 = min(r, c0 + cw);
+  if (active) {
+    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
+      const int rr = e % bi, c = e / bi;
+      ys[e] = double(ybuf[rr + (int64_t)c * ld]);
+    }
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (A.is_lr(bi_, bj_)) {
-    const int r = A.rank[bi_ * A.nb + bj_];
-    const T* U = A.u(bi_, bj_);
-    const T* S = A.s(bi_, bj_);
-    const T* V = A.vt(bi_, bj_);
-    const T* inner = tr ? U : V;      // contracted with y_i (length bi)
-    const T* outer = tr ? V : U;      // expands to length bj
-    for (int cc = wid; cc < r; cc += nw) {
+  // A: t1(c0:c1, :) = inner(:, c0:c1)^T y
+  const T* U = lr ? A.u(bi_, bj_) : nullptr;
+  const T* S = lr ? A.s(bi_, bj_) : nullptr;
+  const T* V = lr ? A.vt(bi_, bj_) : nullptr;
+  const T* inner = tr ? U : V;
+  const T* outer = tr ? V : U;
+  if (lr) {
+    for (int cc = c0 + wid; cc < c1; cc += nw) {
       const T* col = inner + (int64_t)cc * ld;
       double acc[8];
 #pragma unroll
       for (int c = 0; c < 8; ++c) acc[c] = 0.0;
 #pragma unroll 4
-      for (int t = lane; t < bi; t += 32) {
-        const double v = double(col[t]);
+      for (int x = lane; x < bi; x += 32) {
+        const double v = double(col[x]);
 #pragma unroll
         for (int c = 0; c < 8; ++c)
-          if (c < nrhs) acc[c] += v * ys[t + c * bi];
+          if (c < nrhs) acc[c] += v * ys[x + c * bi];
       }
-      for (int c = 0; c < nrhs; ++c) {
+      #pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c >= nrhs) break;
         const double sum = warp_sum(acc[c]);
         if (lane == 0) t1[cc + c * r] = sum;
       }
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < r * nrhs; e += blockDim.x) {
-      const int c = e % r, h = e / r;
-      double sacc = 0.0;
-      for (int t = 0; t < r; ++t) {
-        const double sv = tr ? double(S[t + (int64_t)c * A.kcap]) : double(S[c + (int64_t)t * A.kcap]);
-        sacc += sv * t1[t + h * r];
+  }
+  cl.sync();
+  // B: gather t1, then t2(c0:c1, :) = S(c0:c1, :) t1 (warps split the inner index)
+  if (lr) {
+    for (int qq = 0; qq < SC_CLUSTER; ++qq) {
+      if (qq == q) continue;
+      const int a0 = min(r, qq * cw), a1 = min(r, a0 + cw);
+      const double* rt1 = cl.map_shared_rank(t1, qq);
+      for (int e = threadIdx.x; e < (a1 - a0) * nrhs; e += blockDim.x) {
+        const int c = a0 + e % (a1 - a0), h = e / (a1 - a0);
+        t1[c + h * r] = rt1[c + h * r];
       }
-      t2[c + h * r] = sacc;
     }
     __syncthreads();
-    for (int rr = threadIdx.x; rr < bj; rr += blockDim.x) {
+    const int tw = (r + nw - 1) / nw, x0 = min(r, wid * tw), x1 = min(r, x0 + tw);
+    for (int cb = c0; cb < c1; cb += 32) {
+      const int c = cb + lane;
       double acc[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+      for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+      if (c < c1) {
 #pragma unroll 4
-      for (int t = 0; t < r; ++t) {
-        const double ov = double(outer[rr + (int64_t)t * ld]);
+        for (int x = x0; x < x1; ++x) {
+          const double sv = tr ? double(S[x + (int64_t)c * A.kcap]) : double(S[c + (int64_t)x * A.kcap]);
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < nrhs) acc[c] += ov * t2[t + c * r];
+          for (int h = 0; h < 8; ++h)
+            if (h < nrhs) acc[h] += sv * t1[x + h * r];
+        }
       }
-      for (int c = 0; c < nrhs; ++c) z[oj + rr + (int64_t)c * ldz] = T(double(z[oj + rr + (int64_t)c * ldz]) - acc[c]);
+      if (c < c1)
+        #pragma unroll
+        for (int h = 0; h < 8; ++h) if (h < nrhs) part[((int64_t)wid * pstride + (c - c0)) * 8 + h] = acc[h];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (c1 - c0) * nrhs; e += blockDim.x) {
+      const int cl_ = e % (c1 - c0), h = e / (c1 - c0);
+      double sum = 0.0;
+      for (int w = 0; w < nw; ++w) sum += part[((int64_t)w * pstride + cl_) * 8 + h];
+      t2[c0 + cl_ + h * r] = sum;
+    }
+  }
+  cl.sync();
+  // C: gather t2, then the row tile of the target
+  if (lr) {
+    for (int qq = 0; qq < SC_CLUSTER; ++qq) {
+      if (qq == q) continue;
+      const int a0 = min(r, qq * cw), a1 = min(r, a0 + cw);
+      const double* rt2 = cl.map_shared_rank(t2, qq);
+      for (int e = threadIdx.x; e < (a1 - a0) * nrhs; e += blockDim.x) {
+        const int c = a0 + e % (a1 - a0), h = e / (a1 - a0);
+        t2[c + h * r] = rt2[c + h * r];
+      }
+    }
+  }
+  cl.sync();
+  if (!active) return;
+  const int64_t oj = A.off[j];
+  const int tl = (bj + SC_CLUSTER - 1) / SC_CLUSTER, row0 = q * tl, row1 = min(bj, row0 + tl);
+  if (lr) {
+    // 64 rows x (SOLVE_THREADS / 64) splits of the inner index per pass
+    const int ns = SOLVE_THREADS / 64, rl = threadIdx.x % 64, sl = threadIdx.x / 64;
+    const int xw = (r + ns - 1) / ns, x0 = min(r, sl * xw), x1 = min(r, x0 + xw);
+    for (int rb = row0; rb < row1; rb += 64) {
+      const int rr = rb + rl;
+      double acc[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+      if (rr < row1) {
+#pragma unroll 4
+        for (int x = x0; x < x1; ++x) {
+          const double ov = double(outer[rr + (int64_t)x * ld]);
+#pragma unroll
+          for (int h = 0; h < 8; ++h)
+            if (h < nrhs) acc[h] += ov * t2[x + h * r];
+        }
+      }
+      __syncthreads();
+      #pragma unroll
+      for (int h = 0; h < 8; ++h) if (h < nrhs) part[((int64_t)sl * 64 + rl) * 8 + h] = acc[h];
+      __syncthreads();
+      for (int e = threadIdx.x; e < 64 * nrhs; e += blockDim.x) {
+        const int rl2 = e % 64, h = e / 64, row = rb + rl2;
+        if (row < row1) {
+          double sum = 0.0;
+          for (int w = 0; w < ns; ++w) sum += part[((int64_t)w * 64 + rl2) * 8 + h];
+          z[oj + row + (int64_t)h * ldz] = T(double(z[oj + row + (int64_t)h * ldz]) - sum);
+        }
+      }
     }
   } else {
     const T* Dm = A.dense(bi_, bj_);
     if (!tr) {
-      for (int rr = threadIdx.x; rr < bj; rr += blockDim.x) {
+      for (int rr = row0 + threadIdx.x; rr < row1; rr += blockDim.x) {
         double acc[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+        for (int h = 0; h < 8; ++h) acc[h] = 0.0;
 #pragma unroll 4
-        for (int t = 0; t < bi; ++t) {
-          const double dv = double(Dm[rr + (int64_t)t * ld]);
+        for (int x = 0; x < bi; ++x) {
+          const double dv = double(Dm[rr + (int64_t)x * ld]);
 #pragma unroll
-          for (int c = 0; c < 8; ++c)
-            if (c < nrhs) acc[c] += dv * ys[t + c * bi];
+          for (int h = 0; h < 8; ++h)
+            if (h < nrhs) acc[h] += dv * ys[x + h * bi];
         }
-        for (int c = 0; c < nrhs; ++c) z[oj + rr + (int64_t)c * ldz] = T(double(z[oj + rr + (int64_t)c * ldz]) - acc[c]);
+        #pragma unroll
+        for (int h = 0; h < 8; ++h) if (h < nrhs) z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - acc[h]);
       }
     } else {
-      for (int rr = wid; rr < bj; rr += nw) {
+      for (int rr = row0 + wid; rr < row1; rr += nw) {
         double acc[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = 0.0;
-        for (int t = lane; t < bi; t += 32) {
-          const double dv = double(Dm[t + (int64_t)rr * ld]);
+        for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+        for (int x = lane; x < bi; x += 32) {
+          const double dv = double(Dm[x + (int64_t)rr * ld]);
 #pragma unroll
-          for (int c = 0; c < 8; ++c)
-            if (c < nrhs) acc[c] += dv * ys[t + c * bi];
+          for (int h = 0; h < 8; ++h)
+            if (h < nrhs) acc[h] += dv * ys[x + h * bi];
         }
-        for (int c = 0; c < nrhs; ++c) {
-          const double sum = warp_sum(acc[c]);
-          if (lane == 0) z[oj + rr + (int64_t)c * ldz] = T(double(z[oj + rr + (int64_t)c * ldz]) - sum);
+        #pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          if (h >= nrhs) break;
+          const double sum = warp_sum(acc[h]);
+          if (lane == 0) z[oj + rr + (int64_t)h * ldz] = T(double(z[oj + rr + (int64_t)h * ldz]) - sum);
         }
       }
     }
@@ -1874,6 +1998,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_scatter(BlrView<T> A, i
 // ---------------------------------------------------------------------------
 constexpr int MV_THREADS = 256;
 
+// dynamic shared memory of k_matvec_blocks: x_j (bmax x nrhs), t1, t2 (kcap x nrhs)
+FRANK_HD size_t matvec_smem(int bmax, int kcap, int nrhs) {
+  return ((size_t)bmax * nrhs + 2 * (size_t)kcap * nrhs) * sizeof(double);
+}
+
+// Each element of the block (U, S, V or the dense block) is read once and
+// applied to all nrhs columns of x_j, which is staged in shared memory.
 __global__ void __launch_bounds__(MV_THREADS) k_matvec_blocks(BlrView<double> H, const double* x, int64_t ldx,
                                                               int nrhs, double* part, int transpose) {
   // part(i, j) = A(i, j) x_j, or A(j, i)^T x_j when transposing
@@ -1883,9 +2014,16 @@ __global__ void __launch_bounds__(MV_THREADS) k_matvec_blocks(BlrView<double> H,
   const int64_t oj = H.off[j];
   const int gi = transpose ? j : i, gj = transpose ? i : j;   // stored block (gi, gj)
   double* out = part + (int64_t)(i * nb + j) * ld * nrhs;
-  extern __shared__ double t1[];   // 2 * kcap * nrhs doubles
-  double* t2 = t1 + (int64_t)H.kcap * nrhs;
+  extern __shared__ double msm[];
+  double* xs = msm;                                  // bj x nrhs
+  double* t1 = xs + (int64_t)H.bmax * nrhs;          // r x nrhs
+  double* t2 = t1 + (int64_t)H.kcap * nrhs;          // r x nrhs
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int e = threadIdx.x; e < bj * nrhs; e += blockDim.x) {
+    const int t = e % bj, h = e / bj;
+    xs[e] = x[oj + t + (int64_t)h * ldx];
+  }
+  __syncthreads();
   if (H.is_lr(gi, gj)) {
     const int r = H.rank[gi * nb + gj];
     const double* U = H.u(gi, gj);
@@ -1893,46 +2031,90 @@ __global__ void __launch_bounds__(MV_THREADS) k_matvec_blocks(BlrView<double> H,
     const double* V = H.vt(gi, gj);
     const double* inner = transpose ? U : V;   // length bj (rows of x_j)
     const double* outer = transpose ? V : U;   // length bi
-    for (int e = wid; e < r * nrhs; e += nw) {
-      const int c = e % r, h = e / r;
-      double s = 0.0;
-      for (int t = lane; t < bj; t += 32) s += inner[t + (int64_t)c * ld] * x[oj + t + (int64_t)h * ldx];
-      s = warp_sum(s);
-      if (lane == 0) t1[c + h * r] = s;
+    for (int c = wid; c < r; c += nw) {
+      const double* col = inner + (int64_t)c * ld;
+      double acc[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+#pragma unroll 4
+      for (int t = lane; t < bj; t += 32) {
+        const double v = col[t];
+#pragma unroll
+        for (int h = 0; h < 8; ++h)
+          if (h < nrhs) acc[h] += v * xs[t + h * bj];
+      }
+      #pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        if (h >= nrhs) break;
+        const double sum = warp_sum(acc[h]);
+        if (lane == 0) t1[c + h * r] = sum;
+      }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < r * nrhs; e += blockDim.x) {
-      const int c = e % r, h = e / r;
-      double s = 0.0;
+    for (int c = threadIdx.x; c < r; c += blockDim.x) {
+      double acc[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+#pragma unroll 4
       for (int t = 0; t < r; ++t) {
         const double sv = transpose ? S[t + (int64_t)c * H.kcap] : S[c + (int64_t)t * H.kcap];
-        s += sv * t1[t + h * r];
+#pragma unroll
+        for (int h = 0; h < 8; ++h)
+          if (h < nrhs) acc[h] += sv * t1[t + h * r];
       }
-      t2[c + h * r] = s;
+      #pragma unroll
+      for (int h = 0; h < 8; ++h) if (h < nrhs) t2[c + h * r] = acc[h];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
-      const int rr = e % bi, h = e / bi;
-      double s = 0.0;
-      for (int t = 0; t < r; ++t) s += outer[rr + (int64_t)t * ld] * t2[t + h * r];
-      out[rr + (int64_t)h * ld] = s;
+    for (int rr = threadIdx.x; rr < bi; rr += blockDim.x) {
+      double acc[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+#pragma unroll 4
+      for (int t = 0; t < r; ++t) {
+        const double ov = outer[rr + (int64_t)t * ld];
+#pragma unroll
+        for (int h = 0; h < 8; ++h)
+          if (h < nrhs) acc[h] += ov * t2[t + h * r];
+      }
+      #pragma unroll
+      for (int h = 0; h < 8; ++h) if (h < nrhs) out[rr + (int64_t)h * ld] = acc[h];
     }
   } else {
     const double* Dm = H.dense(gi, gj);
     if (!transpose) {
-      for (int e = threadIdx.x; e < bi * nrhs; e += blockDim.x) {
-        const int rr = e % bi, h = e / bi;
-        double s = 0.0;
-        for (int t = 0; t < bj; ++t) s += Dm[rr + (int64_t)t * ld] * x[oj + t + (int64_t)h * ldx];
-        out[rr + (int64_t)h * ld] = s;
+      for (int rr = threadIdx.x; rr < bi; rr += blockDim.x) {
+        double acc[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+#pragma unroll 4
+        for (int t = 0; t < bj; ++t) {
+          const double dv = Dm[rr + (int64_t)t * ld];
+#pragma unroll
+          for (int h = 0; h < 8; ++h)
+            if (h < nrhs) acc[h] += dv * xs[t + h * bj];
+        }
+        #pragma unroll
+        for (int h = 0; h < 8; ++h) if (h < nrhs) out[rr + (int64_t)h * ld] = acc[h];
       }
     } else {
-      for (int e = wid; e < bi * nrhs; e += nw) {
-        const int rr = e % bi, h = e / bi;
-        double s = 0.0;
-        for (int t = lane; t < bj; t += 32) s += Dm[t + (int64_t)rr * ld] * x[oj + t + (int64_t)h * ldx];
-        s = warp_sum(s);
-        if (lane == 0) out[rr + (int64_t)h * ld] = s;
+      for (int rr = wid; rr < bi; rr += nw) {
+        double acc[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) acc[h] = 0.0;
+#pragma unroll 4
+        for (int t = lane; t < bj; t += 32) {
+          const double dv = Dm[t + (int64_t)rr * ld];
+#pragma unroll
+          for (int h = 0; h < 8; ++h)
+            if (h < nrhs) acc[h] += dv * xs[t + h * bj];
+        }
+        #pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          if (h >= nrhs) break;
+          const double sum = warp_sum(acc[h]);
+          if (lane == 0) out[rr + (int64_t)h * ld] = sum;
+        }
       }
     }
   }
