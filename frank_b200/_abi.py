@@ -47,6 +47,31 @@ SIGNATURES = {
     "frank_device_info": (C.c_int, [C.c_char_p, C.c_int, _ip, _ip, _ip]),
     "frank_blr_create": (C.c_int, [C.POINTER(BlrDesc), C.POINTER(_vp)]),
     "frank_blr_create_geometric": (C.c_int, [C.POINTER(BlrDesc), _dp, C.c_int, C.POINTER(_vp)]),
+    "frank_device_alloc": (C.c_int, [C.c_size_t, C.POINTER(_vp)]),
+    "frank_device_free": (C.c_int, [_vp]),
+    "frank_copy": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int]),
+    "frank_blr_trsm": (C.c_int, [_vp, C.c_int, _dp, C.c_int64, C.c_int, _vp]),
+    "frank_blr_gemv": (C.c_int, [_vp, C.c_double, _dp, C.c_int64, C.c_double, _dp, C.c_int64, C.c_int, _vp]),
+    "frank_gemm_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _vp, C.c_int64, C.c_int64,
+                                     C.c_int, _vp, C.c_int64, C.c_int64, C.c_int, C.c_double, _vp, C.c_int64,
+                                     C.c_int64, _vp]),
+    "frank_qr_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64,
+                                   _vp, C.c_int64, C.c_int64, _vp]),
+    "frank_rq_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64,
+                                   _vp, C.c_int64, C.c_int64, _vp]),
+    "frank_svd_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64,
+                                    _vp, C.c_int64, _vp, C.c_int64, C.c_int64, _vp]),
+    "frank_rsvd_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int64, C.c_int64,
+                                     _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64,
+                                     _vp]),
+    "frank_id_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int64, C.c_int64, _vp, C.c_int64,
+                                   C.c_int64, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64, _vp, _vp, _vp]),
+    "frank_rid_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int64, C.c_int64, _vp,
+                                    C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64, _vp]),
+    "frank_lowrank_add_batched": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_double,
+                                            _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64, _vp, C.c_int64,
+                                            C.c_int64, _vp, _vp, C.c_int64, C.c_int64, _vp, C.c_int64, C.c_int64,
+                                            _vp, C.c_int64, C.c_int64, _vp, C.c_int, _vp]),
     "frank_blr_destroy": (C.c_int, [_vp]),
     "frank_blr_offsets": (C.c_int, [_vp, _i64p]),
     "frank_blr_set_dense": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_int64, C.c_int]),

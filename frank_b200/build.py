@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfrank_b200.so")
-SOURCES = ["api.cu"]
+SOURCES = ["api.cu", "ops.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,11 +40,34 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(f) <= t for f in _deps())
 
 
+CPP_DIR = os.path.join(HERE, "cpp")
+CPP_LIB = os.path.join(LIBDIR, "libfrank_b200_cpp.so")
+
+
+def build_cpp(force: bool = False) -> str:
+    """The C++ layer (namespace FRANK over the C ABI) as libfrank_b200_cpp.so,
+    linked against libfrank_b200.so next to it."""
+    lib = build(force=force)
+    srcs = [os.path.join(CPP_DIR, "frank.cpp")]
+    deps = srcs + [os.path.join(CPP_DIR, "include", "frank_b200", f) for f in ("FRANK.hpp", "multimethod.hpp")]
+    deps.append(os.path.join(HERE, "..", "include", "frank_b200.h"))
+    if not force and os.path.exists(CPP_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(CPP_LIB)
+                                                      for d in deps + [lib]):
+        return CPP_LIB
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-I" + os.path.join(CPP_DIR, "include"), *srcs,
+           "-o", CPP_LIB + ".tmp", "-L" + LIBDIR, "-lfrank_b200", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
+    os.replace(CPP_LIB + ".tmp", CPP_LIB)
+    return CPP_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "--threads", "2",
            "-diag-suppress", "177", *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
@@ -59,3 +82,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_cpp())

@@ -53,6 +53,11 @@ struct DevBuf {
 
 }  // namespace
 
+namespace frank {
+// Error text for the per-operation entry points (ops.cu).
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace frank
+
 struct frank_blr {
   int64_t n = 0;
   int nb = 0, bmax = 0, kcap = 0, precision = 0, fixed_rank = 0;
@@ -118,6 +123,7 @@ struct frank_blr {
     int64_t ld = 0;
     int nrhs = 0;
     bool transpose = false;
+    int part = 0;
     int64_t kernels = 0;
   };
   std::vector<SolveGraph> solve_graphs;
@@ -388,8 +394,9 @@ int run_factor(frank_blr* p, cudaStream_t s) {
 
 // ---- solve --------------------------------------------------------------
 
+// part: 0 both sweeps, 1 the forward sweep only (L), 2 the backward sweep only (U).
 template <typename T>
-int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cudaStream_t s) {
+int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cudaStream_t s, int part = 0) {
   BlrView<T> W = work_view<T>(p);
   FactorWs<T> ws = factor_ws<T>(p);
   T* ybuf = static_cast<T*>(p->stmp);
@@ -403,8 +410,8 @@ int enqueue_solve(frank_blr* p, T* z, int64_t ldz, int nrhs, bool transpose, cud
                                                                                        ybuf, ntarget);
   };
   if (!transpose) {
-    for (int i = 0; i < nb; ++i) step(i, 0, 0, nb - i - 1);
-    for (int i = nb - 1; i >= 0; --i) step(i, 1, 1, i);
+    if (part != 2) for (int i = 0; i < nb; ++i) step(i, 0, 0, nb - i - 1);
+    if (part != 1) for (int i = nb - 1; i >= 0; --i) step(i, 1, 1, i);
   } else {
     for (int i = 0; i < nb; ++i) step(i, 2, 2, nb - i - 1);
     for (int i = nb - 1; i >= 0; --i) step(i, 3, 3, i);
@@ -418,17 +425,18 @@ int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 4096); 
 // Enqueue the launches of one solve of d_b (double, n x nrhs, in place): the
 // FP64 plan solves in place, the mixed plan casts to its FP32 vector, solves
 // and casts back.
-int enqueue_solve_all(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s) {
+int enqueue_solve_all(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s,
+                      int part = 0) {
   for (int c0 = 0; c0 < nrhs; c0 += p->solve_chunk) {
     const int nr = std::min(p->solve_chunk, nrhs - c0);
     double* b = d_b + c0 * ldb;
     if (p->precision == FRANK_PREC_FP64) {
-      int rc = enqueue_solve<double>(p, b, ldb, nr, transpose, s);
+      int rc = enqueue_solve<double>(p, b, ldb, nr, transpose, s, part);
       if (rc) return rc;
     } else {
       float* z = static_cast<float*>(p->z);
       k_cast_copy<float, double><<<grid_for(p->n * nr), 256, 0, s>>>(b, ldb, z, p->n, p->n, nr);
-      int rc = enqueue_solve<float>(p, z, p->n, nr, transpose, s);
+      int rc = enqueue_solve<float>(p, z, p->n, nr, transpose, s, part);
       if (rc) return rc;
       k_cast_copy<double, float><<<grid_for(p->n * nr), 256, 0, s>>>(z, p->n, b, ldb, p->n, nr);
     }
@@ -446,16 +454,17 @@ void drop_solve_graphs(frank_blr* p) {
 // d_b (double, n x nrhs) -> solve in T -> back into d_b.  The 2 nb launches
 // per pass are captured once per (buffer, ld, nrhs, direction) on the plan's
 // private capture stream and replayed as one graph launch on `s`.
-int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s) {
+int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool transpose, cudaStream_t s,
+                      int part = 0) {
   if (!p->factored) return fail(FRANK_ERR_STATE, "solve before getrf");
   frank_blr::SolveGraph* hit = nullptr;
   for (auto& g : p->solve_graphs)
-    if (g.ptr == d_b && g.ld == ldb && g.nrhs == nrhs && g.transpose == transpose) hit = &g;
+    if (g.ptr == d_b && g.ld == ldb && g.nrhs == nrhs && g.transpose == transpose && g.part == part) hit = &g;
   if (!hit) {
     if (!p->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
     if (p->solve_graphs.size() >= 4) drop_solve_graphs(p);
     CUDA_TRY(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_solve_all(p, d_b, ldb, nrhs, transpose, p->cap_stream);
+    int rc = enqueue_solve_all(p, d_b, ldb, nrhs, transpose, p->cap_stream, part);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
     if (rc != FRANK_OK) { if (g) cudaGraphDestroy(g); return rc; }
@@ -466,7 +475,7 @@ int solve_device_impl(frank_blr* p, double* d_b, int64_t ldb, int nrhs, bool tra
     e = cudaGraphInstantiate(&sg.exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("solve graph: ") + cudaGetErrorString(e));
-    sg.ptr = d_b; sg.ld = ldb; sg.nrhs = nrhs; sg.transpose = transpose; sg.kernels = (int64_t)nodes;
+    sg.ptr = d_b; sg.ld = ldb; sg.nrhs = nrhs; sg.transpose = transpose; sg.part = part; sg.kernels = (int64_t)nodes;
     p->solve_graphs.push_back(sg);
     hit = &p->solve_graphs.back();
   }
@@ -1094,6 +1103,55 @@ int frank_blr_solve(frank_blr* p, double* b, int64_t ldb, int nrhs, void* stream
   if (rc == FRANK_OK) {
     cudaError_t e = cudaMemcpy2DAsync(b, ldb * sizeof(double), d, p->n * sizeof(double), p->n * sizeof(double), nrhs,
                                       cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return rc;
+}
+
+int frank_blr_trsm(frank_blr* p, int uplo, double* b, int64_t ldb, int nrhs, void* stream) {
+  if (!p || !b || nrhs < 1 || ldb < p->n || (uplo != FRANK_LOWER && uplo != FRANK_UPPER))
+    return fail(FRANK_ERR_INVALID, "bad trsm arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *d = nullptr, *unused = nullptr;
+  {
+    const int rc0 = host_io(p, nrhs, &d, &unused);
+    if (rc0) return rc0;
+  }
+  CUDA_TRY(cudaMemcpy2DAsync(d, p->n * sizeof(double), b, ldb * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyHostToDevice, s));
+  int rc = solve_device_impl(p, d, p->n, nrhs, false, s, uplo == FRANK_LOWER ? 1 : 2);
+  if (rc == FRANK_OK) {
+    cudaError_t e = cudaMemcpy2DAsync(b, ldb * sizeof(double), d, p->n * sizeof(double), p->n * sizeof(double), nrhs,
+                                      cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return rc;
+}
+
+int frank_blr_gemv(frank_blr* p, double alpha, const double* x, int64_t ldx, double beta, double* y, int64_t ldy,
+                   int nrhs, void* stream) {
+  if (!p || !x || !y || nrhs < 1 || ldx < p->n || ldy < p->n) return fail(FRANK_ERR_INVALID, "bad gemv arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double *dx = nullptr, *dy = nullptr;
+  {
+    const int rc0 = host_io(p, nrhs, &dx, &dy);
+    if (rc0) return rc0;
+  }
+  CUDA_TRY(cudaMemcpy2DAsync(dx, p->n * sizeof(double), x, ldx * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyHostToDevice, s));
+  double* dy0 = p->vtmp;     // beta * y needs the old y on the device
+  CUDA_TRY(cudaMemcpy2DAsync(dy0, p->n * sizeof(double), y, ldy * sizeof(double), p->n * sizeof(double), nrhs,
+                             cudaMemcpyHostToDevice, s));
+  int rc = matvec_device_impl(p, dx, p->n, dy, p->n, nrhs, nullptr, 0, s);
+  if (rc == FRANK_OK) {
+    ++p->solve_launches;
+    k_axpby<<<grid_for(p->n * nrhs), 256, 0, s>>>(alpha, dy, beta, dy0, p->n, nrhs);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(y, ldy * sizeof(double), dy0, p->n * sizeof(double), p->n * sizeof(double), nrhs,
+                            cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = fail(FRANK_ERR_CUDA, cudaGetErrorString(e));
   }

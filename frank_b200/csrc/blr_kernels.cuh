@@ -1679,7 +1679,7 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_recompress_gram(BlrView<T> A, 
 //   x_i = Uinv_i z_i ; z_j -= U(j,i) x_i for j < i.
 // ---------------------------------------------------------------------------
 constexpr int SOLVE_THREADS = 256;
-constexpr int SOLVE_ROWS = 64;   // rows of the diagonal solve per CTA
+constexpr int SOLVE_ROWS = 16;   // rows of the diagonal solve per CTA (16 inner-index slices each)
 
 // y = M * P(z_i) (which 0: Linv, permuted input; 1: Uinv),
 // y = M^T z_i (2: Uinv^T), or y = P^T (Linv^T z_i) (3), into ybuf (ld bmax).
@@ -1688,7 +1688,7 @@ constexpr int SOLVE_ROWS = 64;   // rows of the diagonal solve per CTA
 template <typename T>
 __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, FactorWs<T> ws, int i, const T* z,
                                                               int64_t ldz, int nrhs, int which, T* ybuf) {
-  extern __shared__ double xs[];          // b x nrhs input, then 4 x SOLVE_ROWS x nrhs partials
+  extern __shared__ double xs[];          // b x nrhs input, then the slices' partial sums
   const int b = A.bs(i), ld = A.bmax;
   const int64_t o = A.off[i];
   const T* Mx = (which == 0 || which == 3) ? ws.Linv + (int64_t)i * ld * ld : ws.Uinv + (int64_t)i * ld * ld;
@@ -1703,7 +1703,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve_diag(BlrView<T> A, Fact
   if (which <= 1) {
     // rows r0.. of M x: thread (rl, sl) sums the inner slice sl of row rl
     double* part = xs + (int64_t)b * nrhs;
-    const int rl = threadIdx.x % SOLVE_ROWS, sl = threadIdx.x / SOLVE_ROWS;  // 4 slices
+    const int rl = threadIdx.x % SOLVE_ROWS, sl = threadIdx.x / SOLVE_ROWS;  // SOLVE_THREADS / SOLVE_ROWS slices
     const int nsl = SOLVE_THREADS / SOLVE_ROWS;
     const int tlen = (b + nsl - 1) / nsl;
     const int t0 = sl * tlen, t1 = min(b, t0 + tlen);
@@ -2159,6 +2159,13 @@ __global__ void k_cast_copy(const TS* src, int64_t lds, TD* dst, int64_t ldd, in
 }
 
 // x += T(d)
+// y0 = alpha * y + beta * y0 over n x nrhs (both ld n)
+__global__ void k_axpby(double alpha, const double* y, double beta, double* y0, int64_t n, int nrhs) {
+  const int64_t tot = n * nrhs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x)
+    y0[e] = alpha * y[e] + (beta == 0.0 ? 0.0 : beta * y0[e]);
+}
+
 template <typename TS>
 __global__ void k_axpy_cast(const TS* d, int64_t ldd, double* x, int64_t ldx, int64_t n, int nrhs) {
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * nrhs; e += (int64_t)gridDim.x * blockDim.x) {

@@ -20,6 +20,7 @@
 #ifndef FRANK_B200_H
 #define FRANK_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -182,6 +183,21 @@ int frank_blr_getrf(frank_blr* plan, void* stream);
 int frank_blr_solve(frank_blr* plan, double* b, int64_t ldb, int nrhs, void* stream);
 int frank_blr_solve_device(frank_blr* plan, double* d_b, int64_t ldb, int nrhs, void* stream);
 
+/* One of the two block substitutions of the solve on host buffers, in place:
+ * uplo FRANK_LOWER: b = L^{-1} P b (trsm(L, b, Mode::Lower), the forward
+ * sweep, trsm.cpp:163-174 with the leaf pivots applied); FRANK_UPPER:
+ * b = U^{-1} b (trsm(U, b, Mode::Upper), the backward sweep,
+ * trsm.cpp:136-145).  Replaces trsm(Hierarchical, Dense, Mode)
+ * (operations/BLAS/trsm.cpp:117-125, 40-90). */
+enum { FRANK_LOWER = 0, FRANK_UPPER = 1 };
+int frank_blr_trsm(frank_blr* plan, int uplo, double* b, int64_t ldb, int nrhs, void* stream);
+
+/* y = alpha A_H x + beta y in FP64 on host buffers (column-major, nrhs
+ * columns).  Replaces gemm(Hierarchical, Dense, Dense, alpha, beta)
+ * (operations/BLAS/gemm.cpp:581-615). */
+int frank_blr_gemv(frank_blr* plan, double alpha, const double* x, int64_t ldx, double beta, double* y, int64_t ldy,
+                   int nrhs, void* stream);
+
 /* y = A_H x in FP64 (column-major, nrhs columns).  Replaces
  * gemm(Hierarchical, Dense, Dense, 1, 0) (gemm.cpp:581-615). */
 int frank_blr_matvec(frank_blr* plan, const double* x, int64_t ldx, double* y, int64_t ldy,
@@ -257,6 +273,88 @@ int frank_blr_set_timing(frank_blr* plan, int on);
  * [3] LowRank recompression.  The FLOPs count the reference's call sequence
  * with the LAWN 41 operation counts (no reference counterpart; reporting). */
 int frank_blr_kernel_times(const frank_blr* plan, double* ms, double* flops);
+
+/* ---------------------------------------------------------------------------
+ * Per-operation entry points: FRANK's dense factorizations and low-rank
+ * operations one block at a time, batched.  All matrices are FP64,
+ * column-major, in device memory; matrix b of a batch starts at
+ * ptr + b * stride.  m, n <= 4096 (<= 1024 for the SVD).  Synchronous on
+ * `stream`; scratch comes from the stream-ordered pool.
+ * ------------------------------------------------------------------------- */
+
+/* Device buffers for callers of the per-operation entry points that do not
+ * manage device memory themselves (the C++ layer): allocate, free, and copy
+ * host <-> device (to_device != 0: host to device).  No reference
+ * counterpart (the reference's matrices live in host memory). */
+int frank_device_alloc(size_t bytes, void** out);
+int frank_device_free(void* ptr);
+int frank_copy(void* dst, const void* src, size_t bytes, int to_device);
+
+/* C = alpha op(A) op(B) + beta C, op(A) m x k, op(B) k x n (trans_* != 0:
+ * transposed).  Replaces gemm(Dense, Dense, Dense, alpha, beta, TransA,
+ * TransB) (operations/BLAS/gemm.cpp:126-146: cblas_dgemm). */
+int frank_gemm_batched(int m, int n, int k, int count, double alpha, const double* d_a, int64_t lda, int64_t stride_a,
+                       int trans_a, const double* d_b, int64_t ldb, int64_t stride_b, int trans_b, double beta,
+                       double* d_c, int64_t ldc, int64_t stride_c, void* stream);
+
+/* Householder QR: Q (m x k, explicit), R (k x n, upper trapezoidal), k = min(m, n).
+ * Replaces qr(A, Q, R) (operations/LAPACK/qr.cpp:65-90: dgeqrf + dorgqr). */
+int frank_qr_batched(int m, int n, int count, const double* d_a, int64_t lda, int64_t stride_a, double* d_q,
+                     int64_t ldq, int64_t stride_q, double* d_r, int64_t ldr, int64_t stride_r, void* stream);
+
+/* RQ: A = R Q with R (m x k, upper trapezoidal) and Q (k x n, orthonormal
+ * rows), k = min(m, n).  Replaces rq(A, R, Q) (operations/LAPACK/rq.cpp:43-70:
+ * dgerqf + dorgrq); rows of Q (and columns of R) may differ in sign from
+ * LAPACK's. */
+int frank_rq_batched(int m, int n, int count, const double* d_a, int64_t lda, int64_t stride_a, double* d_r,
+                     int64_t ldr, int64_t stride_r, double* d_q, int64_t ldq, int64_t stride_q, void* stream);
+
+/* Thin SVD by one-sided Jacobi: A = U diag(s) Vt, U (m x k), s (k, descending),
+ * Vt (k x n), k = min(m, n).  Replaces svd(A) (operations/LAPACK/svd.cpp:23-44:
+ * dgesvd 'S','S'; singular vectors up to sign).  FRANK_ERR_NOT_CONVERGED if
+ * the sweeps do not converge. */
+int frank_svd_batched(int m, int n, int count, const double* d_a, int64_t lda, int64_t stride_a, double* d_u,
+                      int64_t ldu, int64_t stride_u, double* d_s, int64_t stride_s, double* d_vt, int64_t ldvt,
+                      int64_t stride_vt, void* stream);
+
+/* Randomized SVD truncated to `rank`: U (m x rank), S (rank x rank, diagonal),
+ * V (rank x n).  Sample rank + oversample (capped at min(m, n)) columns with
+ * the reference's Omega (random_uniform: std::mt19937 seeded 0, uniform [0,1),
+ * functions.cpp:52-66), `power_its` subspace iterations.  Replaces
+ * LowRank(Dense, rank) (classes/low_rank.cpp:40-48: rsvd with oversample 5,
+ * no power iteration, operations/randomized/rsvd.cpp:17-29). */
+int frank_rsvd_batched(int m, int n, int count, int rank, int oversample, int power_its, const double* d_a,
+                       int64_t lda, int64_t stride_a, double* d_u, int64_t ldu, int64_t stride_u, double* d_s,
+                       int64_t lds, int64_t stride_s, double* d_v, int64_t ldv, int64_t stride_v, void* stream);
+
+/* Interpolative decomposition at rank k: A ~= U S V with S = A(rows, cols)
+ * (k x k), U (m x k), V (k x n), rows / cols the selected indices (0-based,
+ * k per matrix), from column-pivoted QR (geqp3) and R11^{-1} R12.  Replaces
+ * id(A, k) (operations/LAPACK/id.cpp:75-116, one_sided_id :49-73). */
+int frank_id_batched(int m, int n, int count, int k, const double* d_a, int64_t lda, int64_t stride_a, double* d_u,
+                     int64_t ldu, int64_t stride_u, double* d_s, int64_t lds, int64_t stride_s, double* d_v,
+                     int64_t ldv, int64_t stride_v, int* d_rows, int* d_cols, void* stream);
+
+/* Randomized ID: the ID of Q^T A at rank k, Q an orthonormal basis of
+ * A Omega (sample columns, the reference's Omega), U = Q U_b.  Replaces
+ * rid(A, sample, k) (operations/randomized/rid.cpp:18-31). */
+int frank_rid_batched(int m, int n, int count, int sample, int k, const double* d_a, int64_t lda, int64_t stride_a,
+                      double* d_u, int64_t ldu, int64_t stride_u, double* d_s, int64_t lds, int64_t stride_s,
+                      double* d_v, int64_t ldv, int64_t stride_v, void* stream);
+
+/* A += B for low-rank pairs, in place on A: A = Ua Sa Va (m x ka, ka x ka,
+ * ka x n, capacity kmax), B = Ub Sb Vb (kb <= kb_max); ranks d_ka (in/out) and
+ * d_kb per pair.  lra "rounded_addition" (addition.cpp:93-127: QR of both
+ * stacked bases, core SVD, rank by find_svd_truncation_rank at eps, or ka when
+ * eps = 0) or "fast_rounded_addition" (addition.cpp:133-189: fixed rank, A's
+ * bases orthonormal; falls back to rounded_addition when eps > 0).  Replaces
+ * operator+=(LowRank&, const LowRank&) (addition.cpp:191-203). */
+int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra, double eps, double* d_ua,
+                              int64_t ldua, int64_t stride_ua, double* d_sa, int64_t ldsa, int64_t stride_sa,
+                              double* d_va, int64_t ldva, int64_t stride_va, int* d_ka, const double* d_ub,
+                              int64_t ldub, int64_t stride_ub, const double* d_sb, int64_t ldsb, int64_t stride_sb,
+                              const double* d_vb, int64_t ldvb, int64_t stride_vb, const int* d_kb, int kb_max,
+                              void* stream);
 
 /* Largest block order accepted by frank_getrf_dense_noalloc. */
 #define FRANK_NOALLOC_MAX_N 256

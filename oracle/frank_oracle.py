@@ -950,3 +950,52 @@ def blr_ranks(H) -> List[Tuple[int, int, int]]:
             if isinstance(H[i, j], LowRank):
                 out.append((i, j, H[i, j].rank))
     return out
+
+
+# --------------------------------------------------------------------------
+# Interpolative decompositions (operations/LAPACK/id.cpp, randomized/rid.cpp)
+# --------------------------------------------------------------------------
+
+
+def geqp3(A: np.ndarray):
+    """operations/LAPACK/geqp3.cpp:36-69: LAPACKE_dgeqp3 with jpvt = 0 (all
+    columns free); returns R (the upper triangle of the factored matrix,
+    n x n) and the 0-based column order."""
+    m, n = A.shape
+    qr_, jpvt, tau, work, info = lapack.dgeqp3(np.asfortranarray(A.copy()), np.zeros(n, dtype=np.int32))
+    R = np.zeros((n, n))
+    k = min(m, n)
+    R[:k, :] = np.triu(qr_[:k, :])
+    return R, [int(j) - 1 for j in jpvt]
+
+
+def one_sided_id(A: np.ndarray, k: int):
+    """operations/LAPACK/id.cpp:49-73: V (k x n) with A ~= A[:, cols] V."""
+    m, n = A.shape
+    R, P = geqp3(A)
+    if k < min(m, n) or n > m:
+        T = trsm_dense(R[:k, :k], R[:k, k:], upper=True, left=True)
+    else:
+        T = np.zeros((k, 0))
+    V = np.zeros((k, n))
+    for j in range(n):                                   # interleave_id (id.cpp:29-39)
+        V[:, P[j]] = np.eye(k)[:, j] if j < k else T[:, j - k]
+    return V, P[:k]
+
+
+def id_(A: np.ndarray, k: int):
+    """operations/LAPACK/id.cpp:100-111: A ~= U S V with S = A[rows, cols]."""
+    V, cols = one_sided_id(A.copy(), k)
+    AC = A[:, cols]
+    Ut, rows = one_sided_id(AC.T.copy(), k)
+    return Ut.T.copy(), AC[rows, :].copy(), V, rows, cols
+
+
+def rid(A: np.ndarray, sample: int, k: int):
+    """operations/randomized/rid.cpp:18-31 with the reference's Omega."""
+    m, n = A.shape
+    RN = random_uniform(n, sample)
+    Y = gemm(A, RN)
+    Q, _ = qr_dense(Y)
+    U, S, V, _, _ = id_(gemm(Q, A, 1.0, True, False), k)
+    return gemm(Q, U), S, V
