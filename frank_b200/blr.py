@@ -215,6 +215,11 @@ class BLRMatrix:
               "frank_blr_refine_device")
         return it.value, res.value
 
+    def write_json(self, path: str, which: int = 0):
+        """The block tree with per-block singular values, in the layout of
+        FRANK's write_JSON (util/print.cpp:54-128)."""
+        check(lib().frank_blr_write_json(self._h, int(which), str(path).encode()), "frank_blr_write_json")
+
     def set_grid(self, ctas: int):
         """Limit the update / recompression grids to `ctas` thread blocks
         (plans that run concurrently in a batch); every target then runs on

@@ -1217,6 +1217,89 @@ int frank_blr_refine(frank_blr* p, const double* b, int64_t ldb, double* x, int6
   return rc;
 }
 
+int frank_blr_write_json(const frank_blr* p, int which, const char* path) {
+  if (!p || !path || (which != 0 && which != 1)) return fail(FRANK_ERR_INVALID, "bad write_json arguments");
+  if (which == 1 && (!p->factored || p->precision != FRANK_PREC_FP64))
+    return fail(FRANK_ERR_UNSUPPORTED, "write_json of the factor needs a factored FP64 plan");
+  const int nb = p->nb, bm = p->bmax, kc = p->kcap;
+  const double* D = which ? static_cast<const double*>(p->Wd) : p->Hd;
+  const double* U = which ? static_cast<const double*>(p->Wu) : p->Hu;
+  const double* S = which ? static_cast<const double*>(p->Ws) : p->Hs;
+  const double* V = which ? static_cast<const double*>(p->Wv) : p->Hv;
+  const int* rk = which ? p->d_rankW : p->d_rankH;
+  std::vector<int> ranks((size_t)nb * nb);
+  CUDA_TRY(cudaMemcpy(ranks.data(), rk, sizeof(int) * ranks.size(), cudaMemcpyDeviceToHost));
+  // scratch: U / Vt factors of an SVD (bm x bm each), singular values, the
+  // small core products (kc x kc each)
+  DevBuf<double> su, ss, sv, qa, ra, qb, rb, t1, t2;
+  CUDA_TRY(su.alloc((size_t)bm * bm));
+  CUDA_TRY(ss.alloc((size_t)bm));
+  CUDA_TRY(sv.alloc((size_t)bm * bm));
+  CUDA_TRY(qa.alloc((size_t)bm * kc));
+  CUDA_TRY(ra.alloc((size_t)kc * kc));
+  CUDA_TRY(qb.alloc((size_t)bm * kc));
+  CUDA_TRY(rb.alloc((size_t)kc * kc));
+  CUDA_TRY(t1.alloc((size_t)kc * kc));
+  CUDA_TRY(t2.alloc((size_t)kc * kc));
+  std::string out;
+  char buf[64];
+  auto num = [&](double v) { snprintf(buf, sizeof buf, "%.17g", v); out += buf; };
+  const int64_t n = p->n;
+  out += "{\"abs_pos\":[0,0],\"children\":[";
+  for (int i = 0; i < nb; ++i) {
+    out += i ? ",[" : "[";
+    for (int j = 0; j < nb; ++j) {
+      const int bi = p->off_h[i + 1] - p->off_h[i], bj = p->off_h[j + 1] - p->off_h[j], k = std::min(bi, bj);
+      std::vector<double> sval(k, 0.0);
+      const int ls = p->lslot_h[i * nb + j];
+      int rc = FRANK_OK;
+      const int r = ls >= 0 ? ranks[i * nb + j] : 0;
+      if (ls < 0) {
+        rc = frank_svd_batched(bi, bj, 1, D + (size_t)p->dslot_h[i * nb + j] * bm * bm, bm, 0, su.get(), bi, 0,
+                               ss.get(), 0, sv.get(), k, 0, nullptr);
+        if (rc == FRANK_OK) CUDA_TRY(cudaMemcpy(sval.data(), ss.get(), sizeof(double) * k, cudaMemcpyDeviceToHost));
+      } else if (r > 0) {
+        // singular values of U S V from its core R_u S R_v^T (QR of both bases)
+        const double* u = U + (size_t)ls * bm * kc;
+        const double* vt = V + (size_t)ls * bm * kc;
+        const double* sm = S + (size_t)ls * kc * kc;
+        rc = frank_qr_batched(bi, r, 1, u, bm, 0, qa.get(), bi, 0, ra.get(), r, 0, nullptr);
+        if (rc == FRANK_OK) rc = frank_qr_batched(bj, r, 1, vt, bm, 0, qb.get(), bj, 0, rb.get(), r, 0, nullptr);
+        if (rc == FRANK_OK)
+          rc = frank_gemm_batched(r, r, r, 1, 1.0, ra.get(), r, 0, 0, sm, kc, 0, 0, 0.0, t1.get(), r, 0, nullptr);
+        if (rc == FRANK_OK)
+          rc = frank_gemm_batched(r, r, r, 1, 1.0, t1.get(), r, 0, 0, rb.get(), r, 0, 1, 0.0, t2.get(), r, 0, nullptr);
+        if (rc == FRANK_OK)
+          rc = frank_svd_batched(r, r, 1, t2.get(), r, 0, su.get(), r, 0, ss.get(), 0, sv.get(), r, 0, nullptr);
+        if (rc == FRANK_OK) CUDA_TRY(cudaMemcpy(sval.data(), ss.get(), sizeof(double) * r, cudaMemcpyDeviceToHost));
+      }
+      if (rc != FRANK_OK) return rc;
+      out += j ? ",{" : "{";
+      snprintf(buf, sizeof buf, "\"abs_pos\":[%d,%d],\"dim\":[%d,%d],\"level\":1,", i, j, bi, bj);
+      out += buf;
+      if (ls >= 0) {
+        snprintf(buf, sizeof buf, "\"rank\":%d,", r);
+        out += buf;
+      }
+      out += "\"svalues\":[";
+      for (int c = 0; c < k; ++c) {
+        if (c) out += ",";
+        num(sval[c]);
+      }
+      out += ls >= 0 ? "],\"type\":\"LowRank\"}" : "],\"type\":\"Dense\"}";
+    }
+    out += "]";
+  }
+  snprintf(buf, sizeof buf, "],\"dim\":[%lld,%lld],\"level\":0,\"type\":\"Hierarchical\"}", (long long)n, (long long)n);
+  out += buf;
+  FILE* f = fopen(path, "w");
+  if (!f) return fail(FRANK_ERR_INVALID, std::string("cannot write ") + path);
+  const size_t w = fwrite(out.data(), 1, out.size(), f);
+  fclose(f);
+  if (w != out.size()) return fail(FRANK_ERR_INVALID, std::string("short write to ") + path);
+  return FRANK_OK;
+}
+
 int frank_blr_kernel_times(const frank_blr* p, double* ms, double* flops) {
   if (!p) return fail(FRANK_ERR_INVALID, "null plan");
   // four reported classes; the inverse kernel's time belongs to class 0

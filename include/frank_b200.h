@@ -255,6 +255,17 @@ int frank_batch_getrf(frank_batch* batch, void* stream);
 int frank_batch_refine_device(frank_batch* batch, const double* const* d_b, int64_t ldb, double* const* d_x,
                               int64_t ldx, int nrhs, double tol, int maxit, int* iters, double* resid);
 
+/* Write the block tree of A_H (which = 0) or of the factor (which = 1, FP64
+ * plans after getrf) as JSON in the layout of FRANK's write_JSON
+ * (util/print.cpp:54-128, keys sorted as nlohmann::json prints them): the
+ * Hierarchical root with "abs_pos", "children" (rows of blocks), "dim",
+ * "level", "type"; every block with its "abs_pos", "dim", "level", "type",
+ * its singular values "svalues" (min(m, n) of them, computed on the GPU;
+ * those of a LowRank block beyond its rank are 0) and, for LowRank blocks,
+ * "rank".  Replaces write_JSON(const Matrix&, filename)
+ * (util/print.cpp:124-128). */
+int frank_blr_write_json(const frank_blr* plan, int which, const char* path);
+
 /* Counters of the last getrf: kernels launched by it plus those of every
  * solve / matvec / refine since, recompressions performed, the largest
  * recompressed rank and the number of ranks clamped at max_rank. */

@@ -22,6 +22,7 @@
 //   [--kparams p0,p1] [--points FILE --dim D] [--rhs FILE --nrhs K]
 //   [--admis-type position|geometry] [--residual] [--factor-error]
 //   [--dump-factor FILE] [--dump-x FILE] [--threads T] [--repeat R] [--no-solve]
+//   [--write-json FILE]   (write_JSON of A_H, util/print.cpp:124-128)
 #include "FRANK/FRANK.h"
 
 #include <cblas.h>
@@ -77,7 +78,7 @@ struct Args {
   int64_t n = 0, nb = 0, rank = 0, nleaf = 0, nrhs = 1;
   double eps = 0.0, admis = 0.0;
   int dim = 1, threads = 0, repeat = 1;
-  std::string lra, kernel = "laplace", points, rhs, dump_factor, dump_x;
+  std::string lra, kernel = "laplace", points, rhs, dump_factor, dump_x, write_json;
   bool residual = false, factor_error = false, solve = true, geometry = false;
 };
 
@@ -116,6 +117,7 @@ Args parse(int argc, char** argv) {
     else if (f == "--threads") a.threads = std::atoi(val().c_str());
     else if (f == "--repeat") a.repeat = std::atoi(val().c_str());
     else if (f == "--no-solve") a.solve = false;
+    else if (f == "--write-json") a.write_json = val();
     else if (f == "--admis-type") {
       const std::string v = val();
       if (v == "geometry") a.geometry = true;
@@ -258,6 +260,7 @@ int main(int argc, char** argv) {
                               : Hierarchical(kernel, x, a.n, a.n, a.nleaf, a.eps, a.admis, a.nb, a.nb, at);
   const double t_build = seconds_since(t0);
   const std::vector<int64_t> ranks_h = block_ranks(A);
+  if (!a.write_json.empty()) write_JSON(A, a.write_json);
 
   // right-hand sides: b = A x with x = random_uniform (the tests' choice) or from a file
   Dense xtrue, b;

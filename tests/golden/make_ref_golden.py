@@ -11,6 +11,9 @@ oracle/build_ref.py, driven through FRANK's public API (oracle/ref_driver.cpp)
   l2_error(x, x_hat) for b = A_H x with the reference's x = random_uniform,
   residual, factorization error ||A_H V - L U V|| / ||A_H V|| on random
   probes, and the per-block ranks of A_H, L and U;
+* reference_json_n256.json: write_JSON (util/print.cpp:124-128) of the
+  Laplace-1D N=256 matrix in 4 x 4 blocks at eps 1e-8 (block tree and
+  per-block singular values);
 * reference_vectors.npz: for the fixed-rank Laplace-1D N=2048 workload (8 x 8
   blocks of 256, rank 16; both LowRank additions) and the leading 8 x 8 blocks
   (N=4096) of the headline Laplace-3D point set at eps 1e-8 (4 RHS): the
@@ -142,6 +145,11 @@ def main():
                                        "--points", px, "--dim", 3, "--rhs", pb, "--nrhs", 4], wd, vec, a.threads)
         vec[tag + "/points_checksum"] = np.array([x.sum(), (x * x).sum()])
         vec[tag + "/rhs_checksum"] = np.array([b.sum(), (b * b).sum()])
+    with tempfile.TemporaryDirectory(dir=a.workdir) as wd:
+        pj = os.path.join(wd, "h.json")
+        run(["--n", 256, "--nb", 4, "--eps", 1e-8, "--no-solve", "--write-json", pj])
+        with open(pj) as f, open(os.path.join(HERE, "reference_json_n256.json"), "w") as g:
+            g.write(f.read())
     with open(os.path.join(HERE, "reference_blr.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_ref_golden.py (oracle/_ref/frank_ref)", "cases": cases,
                    "vectors_meta": meta}, f, indent=0)

@@ -200,3 +200,33 @@ def test_headline4096_mixed_refined_matches_reference(gpu_lib, headline4096, lra
     assert _rel(xs, h["xd"]) <= max(ERR_FACTOR * ref_err, 1e-9)
     assert _rel(xs, xr) <= 10 * 1e-8
     M.close()
+
+
+def test_write_json_matches_reference(gpu_lib, tmp_path):
+    """frank_blr_write_json against the reference's write_JSON of the same
+    matrix (Laplace-1D N=256, 4 x 4 blocks, eps 1e-8): same tree, types,
+    dimensions, positions, levels and ranks; singular values to 1e-12 of the
+    block's largest (dense blocks) or 1e-10 (low-rank blocks, whose values
+    beyond the rank are 0 here and roundoff in the reference)."""
+    ref = json.load(open(os.path.join(GOLD, "reference_json_n256.json")))
+    n, nb = 256, 4
+    x = np.array([fo.get_sorted_random_vector(n)])
+    A = fo.build_hierarchical(fo.laplacend, x, n, n // nb, nb, eps=1e-8)
+    M = _plan(A, n, nb, admis=0.0, admis_type="position", x=x, eps=1e-8)
+    out = tmp_path / "h.json"
+    M.write_json(str(out))
+    got = json.load(open(out))
+    assert list(got.keys()) == list(ref.keys())
+    for k in ("abs_pos", "dim", "level", "type"):
+        assert got[k] == ref[k]
+    for i in range(nb):
+        for j in range(nb):
+            g, r = got["children"][i][j], ref["children"][i][j]
+            assert list(g.keys()) == list(r.keys())
+            for k in ("abs_pos", "dim", "level", "type") + (("rank",) if "rank" in r else ()):
+                assert g[k] == r[k], (i, j, k)
+            gs, rs = np.array(g["svalues"]), np.array(r["svalues"])
+            assert gs.shape == rs.shape
+            tol = 1e-10 if r["type"] == "LowRank" else 1e-12
+            np.testing.assert_allclose(gs, rs, rtol=0, atol=tol * rs[0])
+    M.close()
