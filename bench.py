@@ -234,6 +234,57 @@ def fp64_gemm_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
+def fp32_gemm_peak(torch):
+    """Measured cuBLAS FP32 GEMM throughput (TFLOP/s, TF32 off): the roofline
+    denominator of the mixed plan's FP32 classes."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(3):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+            best = min(best, s.elapsed_time(e) / 1e3)
+        del a, b
+        return 2.0 * n ** 3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def hbm_peak():
+    """Measured copy bandwidth (GB/s) of MEASURED_PEAKS.json, else the
+    pool's earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def plan_bytes(M, which, elem):
+    """Bytes of the blocks of A_H (which 0) or of the factor (1): dense blocks
+    b_i b_j, low-rank blocks U, S, V at their ranks; `elem` bytes per value."""
+    nb = M.nb
+    tot = 0
+    for i in range(nb):
+        for j in range(nb):
+            bi, bj = M.block_size(i), M.block_size(j)
+            if M.is_lowrank(i, j):
+                r = M.rank(i, j, which)
+                tot += (bi * r + r * r + bj * r) * elem
+            elif which == 0 or i != j:
+                tot += bi * bj * elem
+    if which == 1:
+        tot += sum(2 * M.block_size(i) ** 2 * elem for i in range(nb))   # explicit inverses of the diagonal factors
+    return tot
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -250,7 +301,12 @@ def run_ours(args, rank, world):
     stream = torch.cuda.current_stream().cuda_stream
 
     arms = {}
-    for prec, feps in (("mixed", c["mixed_eps"]), ("fp64", c["eps"])):
+    # mixed: FP32 factor at the loose tolerance; fp64: FP64 factor at the
+    # workload's tolerance; fp64_at_mixed_eps (control): FP64 factor at the
+    # mixed arm's tolerance, so the precision gain is seen apart from the
+    # tolerance gain.  All three refine in FP64 to the same residual.
+    for arm, prec, feps in (("mixed", "mixed", c["mixed_eps"]), ("fp64", "fp64", c["eps"]),
+                            ("fp64_at_mixed_eps", "fp64", c["mixed_eps"])):
         M = BLRMatrix(c["n"], c["nb"], eps=feps, precision=prec)
         M.build_kernel(c["kernel"], x, c["eps"])
         torch.cuda.synchronize()
@@ -266,7 +322,7 @@ def run_ours(args, rank, world):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        clk = Clocks(dev) if (rank == 0 and prec == "mixed") else None
+        clk = Clocks(dev) if (rank == 0 and arm == "mixed") else None
         times, its, ress, kt = [], [], [], []
         for _ in range(args.steps):
             s = torch.cuda.Event(enable_timing=True)
@@ -295,25 +351,67 @@ def run_ours(args, rank, world):
         M.getrf()
         M.refine(b_host, tol=c["tol"], maxit=60)
         e2e = []
-        for _ in range(max(1, min(args.steps, 3))):
+        for _ in range(max(1, min(args.steps, 3)) if arm != "fp64_at_mixed_eps" else 0):
             t0 = time.perf_counter()
             M.getrf()
             xs, it_h, res_h = M.refine(b_host, tol=c["tol"], maxit=60)
             e2e.append(time.perf_counter() - t0)
         st = M.stats()
+        # one solve and one FP64 H-matvec, timed alone (the HBM-bound classes)
+        z = b_dev.clone()
+        y = torch.zeros_like(b_dev)
+
+        def ev(f, reps=3):
+            ts_ = []
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s_.record(); f(); e_.record(); e_.synchronize()
+                ts_.append(s_.elapsed_time(e_))
+            return statistics.median(ts_)
+        solve_ms = ev(lambda: M.solve_device(z.data_ptr(), c["nrhs"], stream=stream))
+        matvec_ms = ev(lambda: M.matvec_device(b_dev.data_ptr(), y.data_ptr(), c["nrhs"], stream=stream))
+        elem = 8 if prec == "fp64" else 4
         ranks = [M.rank(i, j, 1) for i in range(c["nb"]) for j in range(c["nb"]) if i != j]
-        arms[prec] = dict(times=times, its=its, res=ress, kt=kt, e2e=e2e, clocks=clocks, stats=st,
-                          mean_rank=float(np.mean(ranks)), max_rank=int(max(ranks)))
+        arms[arm] = dict(times=times, its=its, res=ress, kt=kt, e2e=e2e, clocks=clocks, stats=st,
+                         mean_rank=float(np.mean(ranks)), max_rank=int(max(ranks)), prec=prec, factor_eps=feps,
+                         solve_ms=solve_ms, matvec_ms=matvec_ms, solve_bytes=plan_bytes(M, 1, elem),
+                         matvec_bytes=plan_bytes(M, 0, 8))
         M.close()
         torch.cuda.synchronize()
 
     sample_ours = run_ours_sample(stream, 3)
-    peak64 = fp64_gemm_peak(torch)
+    peaks = dict(fp64=fp64_gemm_peak(torch), fp32=fp32_gemm_peak(torch))
     # max over ranks of the per-step times
-    for prec in arms:
-        arms[prec]["times"] = max_over_ranks(arms[prec]["times"], world, "cuda")
-        arms[prec]["e2e"] = max_over_ranks(arms[prec]["e2e"], world, "cuda")
-    return arms, peak64, sample_ours
+    for arm in arms:
+        arms[arm]["times"] = max_over_ranks(arms[arm]["times"], world, "cuda")
+        if arms[arm]["e2e"]:
+            arms[arm]["e2e"] = max_over_ranks(arms[arm]["e2e"], world, "cuda")
+    return arms, peaks, sample_ours
+
+
+def kernel_roofline(arm, peaks, hbm):
+    """Per kernel class: achieved against its bound.  Compute classes: the
+    reference's algorithmic FLOPs (in-kernel counters, LAWN 41 counts) over
+    the class's device time, against the measured FP64 or FP32 GEMM peak
+    (the arithmetic the class runs in: the leaf LU and the recompression's
+    QR / core are FP64 in both plans, panels and dense updates follow the
+    plan).  HBM classes: the bytes of the blocks one solve / matvec reads
+    over its time, against the measured copy bandwidth."""
+    kt = arm["kt"][-1]
+    work = "fp64" if arm["prec"] == "fp64" else "fp32"
+    out = {}
+    for cls, pipe in (("getrf", "fp64"), ("panel", work), ("dense_update", work), ("recompress", "fp64")):
+        ms, fl = kt[cls]["ms"], kt[cls]["flops"]
+        ach = fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+        out[cls] = {"ms": ms, "achieved": ach, "unit": "TFLOP/s", "peak": peaks[pipe], "frac": ach / peaks[pipe],
+                    "bound": "compute (%s, SIMT)" % pipe}
+    for cls, key in (("solve", "solve"), ("matvec", "matvec")):
+        ms, by = arm[key + "_ms"], arm[key + "_bytes"]
+        ach = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        out[cls] = {"ms": ms, "achieved": ach, "unit": "GB/s", "peak": hbm, "frac": ach / hbm, "bound": "hbm",
+                    "bytes": by}
+    return out
 
 
 # The bounded sample of the workload that the CPU reference runs: the leading
@@ -413,6 +511,14 @@ def run_ours_sample(stream, steps):
         out[arm] = statistics.median(ts)
         M.close()
     return out
+
+
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# k_recompress launch measured by ncu on the profile case (`--profile-case
+# n8192`, the mixed factor at the headline's tolerance), in bytes, and the
+# same launch's algorithmic FLOPs: the per-launch figures behind the roofline
+# (profiles/k_recompress_blr_laplace3d_n8192.md).  None until captured.
+RECOMP_TRAFFIC = None
 
 
 def profile_case(name):
@@ -559,12 +665,15 @@ def main():
         if args.impl == "reference":
             bench_reference(args, rank, world)
             return
-        arms, peak64, sample_ours = run_ours(args, rank, world)
+        arms, peaks, sample_ours = run_ours(args, rank, world)
+        peak64 = peaks["fp64"]
+        hbm, hbm_src = hbm_peak()
         if rank != 0:
             return
-        mx, fp = arms["mixed"], arms["fp64"]
+        mx, fp, ctl = arms["mixed"], arms["fp64"], arms["fp64_at_mixed_eps"]
         t_mixed = statistics.median(mx["times"])
         t_fp64 = statistics.median(fp["times"])
+        t_ctl = statistics.median(ctl["times"])
         kt = mx["kt"][-1]
         rec = kt["recompress"]
         achieved = rec["flops"] / (rec["ms"] / 1e3) / 1e12 if rec["ms"] > 0 else 0.0
@@ -580,12 +689,22 @@ def main():
                      "mean_rank": fp["mean_rank"], "max_rank": fp["max_rank"], "kernel_ms": fp["kt"][-1]},
             "mixed": {"iters": mx["its"][-1], "residual": mx["res"][-1], "mean_rank": mx["mean_rank"],
                       "max_rank": mx["max_rank"], "kernel_ms": kt},
+            "fp64_at_mixed_eps": {"value": t_ctl, "unit": "s", "factor_eps": CFG["mixed_eps"],
+                                  "iters": ctl["its"][-1], "residual": ctl["res"][-1], "mean_rank": ctl["mean_rank"],
+                                  "max_rank": ctl["max_rank"], "kernel_ms": ctl["kt"][-1]},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "speedup_precision_only": t_ctl / t_mixed,
+            "kernel_roofline": {a: kernel_roofline(arms[a], peaks, hbm) for a in ("mixed", "fp64")},
+            "peaks": {"fp64_tflops": peaks["fp64"], "fp32_tflops": peaks["fp32"], "hbm_gbs": hbm,
+                      "source": "cuBLAS DGEMM / SGEMM (TF32 off) 8192^3 measured in this run; HBM " + hbm_src},
             "e2e": {"value": statistics.median(mx["e2e"]), "unit": "s", "fp64_value": statistics.median(fp["e2e"]),
                     "h2d_bytes_per_step": n * nrhs * 8, "d2h_bytes_per_step": n * nrhs * 8},
-            "roofline": {"kernel": "k_recompress (mixed factor)", "bound": "tensor", "achieved": achieved,
-                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64 if peak64 else None,
-                         "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run", "traffic": None},
+            "roofline": {"kernel": "k_recompress (mixed factor)", "bound": "compute (fp64, SIMT)",
+                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                         "frac": achieved / peak64 if peak64 else None,
+                         "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in "
+                                        "MEASURED_PEAKS.json)",
+                         "traffic": RECOMP_TRAFFIC},
             "gpu_launches": mx["stats"]["launches"],
             "clocks": mx["clocks"],
         }

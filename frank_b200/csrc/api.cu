@@ -86,6 +86,7 @@ struct frank_blr {
   int grid_dense = 0, grid_recomp = 0, smax = 0;
   int core_method = CORE_RRQR;   // core of tolerance plans
   int core_fixed = CORE_FAST;    // core of fixed-rank plans (FRANK_LRA unset: fast_rounded_addition)
+  bool proj_tol = false;         // tolerance plans: projected bases (QR of the update's remainder only)
   double core_scale = 0.1;
   int grid_gram = 0;
   double gram_tol = 1e-12;
@@ -318,13 +319,14 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
         ++launches;
         if (p->dense_offdiag) {
           k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr);
+              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr, 0);
           ++launches;
         }
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
             W, ws, i, p->smax, p->fixed_rank > 0 ? p->core_fixed : p->core_method, p->core_scale, 0, p->work + i,
-            p->rsplit ? p->nsplit : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr);
+            p->rsplit ? p->nsplit : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr,
+            p->proj_tol ? 1 : 0);
         ++launches;
       }
     }
@@ -1029,11 +1031,16 @@ int frank_blr_set_lra(frank_blr* p, const char* name, double core_scale) {
   // addition.cpp:191-203: "rounded_addition" selects it for every plan; any
   // other value selects fast_rounded_addition, which falls back to
   // rounded_addition on tolerance plans (addition.cpp:138-143)
+  bool proj = false;
   if (n == "rounded_addition") { p->core_method = CORE_SVD; p->core_fixed = CORE_SVD; p->gram = false; }
   else if (n == "fast_rounded_addition") { p->core_method = CORE_SVD; p->core_fixed = CORE_FAST; p->gram = false; }
   else if (n == "rounded_addition_rrqr") { p->core_method = CORE_RRQR; p->core_fixed = CORE_SVD; p->gram = false; }
+  else if (n == "rounded_addition_rrqr_proj") {
+    p->core_method = CORE_RRQR; p->core_fixed = CORE_FAST; p->gram = false; proj = true;
+  }
   else if (n == "rounded_addition_rrqr_gram") { p->core_method = CORE_RRQR; p->core_fixed = CORE_SVD; p->gram = true; }
   else return fail(FRANK_ERR_UNSUPPORTED, "unknown FRANK_LRA value: " + n);
+  p->proj_tol = proj;
   p->core_scale = core_scale > 0.0 ? core_scale : 0.1;
   if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
   if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }

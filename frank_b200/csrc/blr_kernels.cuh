@@ -1020,7 +1020,7 @@ template <typename T>
 __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
                                                                int core_method, double core_scale,
                                                                int only_dense_operands, int* counter, int nsplit,
-                                                               double* split_base, int* split_done) {
+                                                               double* split_base, int* split_done, int proj_tol) {
   extern __shared__ double dsm[];
   double* gsm = dsm;
   double* region = dsm + RECOMP_GSM;
@@ -1063,7 +1063,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     const int ic = i + 1 + a_, k = i + 1 + c_;
     if (!A.is_lr(ic, k)) continue;
     if (only_dense_operands && A.is_lr(ic, i) && A.is_lr(i, k)) continue;
-    const bool split_t = tsk < nspl && core_method != CORE_FAST && A.is_lr(ic, i) && A.is_lr(i, k) &&
+    const bool split_t = tsk < nspl && A.is_lr(ic, i) && A.is_lr(i, k) &&
                          max(A.rank[ic * A.nb + i], A.rank[i * A.nb + k]) > SPLIT_P;
     if ((side >= 0) != split_t) continue;
     set_base(side >= 0 ? split_base + (int64_t)tsk * ws.rscratch_stride : cta_base);
@@ -1106,89 +1106,36 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     if (do_u) form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
     SUB_MARK(10);
     PHASE_MARK(cls, 0);
-    // fast rounded addition (addition.cpp:133-189) for fixed-rank targets
-    // whose stacked bases fit the block (kc + p <= bc, kc + q <= bk); the
-    // target's U_C, V_C have orthonormal columns (rsvd construction or an
-    // earlier SVD-core recompression)
-    const bool fast = core_method == CORE_FAST && ws.fixed_rank > 0 && side < 0 && kc > 0 && o.p > 0 && o.q > 0 &&
-                      !o.left_dense && !o.right_dense && su <= bc && sv <= bk;
-    if (fast) {
-      const int mu = su, mv = sv;   // kc + p, kc + q
-      // Zu = U_C^T U_B into Rc(0:kc, kc:su), Yu = U_B - U_C Zu in place
-      cta_gemm<double, RECOMP_THREADS>(kc, o.p, bc, 1.0, Ash, bc, true, Ash + (int64_t)kc * bc, bc, false, 0.0,
-                                       Rc + (int64_t)kc * mu, mu, gsm);
-      cta_gemm<double, RECOMP_THREADS>(bc, o.p, kc, -1.0, Ash, bc, false, Rc + (int64_t)kc * mu, mu, false, 1.0,
-                                       Ash + (int64_t)kc * bc, bc, gsm);
-      // Zv = V_C^T V_B (ZvT of the reference transposed), Yv = V_B - V_C Zv
-      cta_gemm<double, RECOMP_THREADS>(kc, o.q, bk, 1.0, Bsh, bk, true, Bsh + (int64_t)kc * bk, bk, false, 0.0,
-                                       Rv + (int64_t)kc * mv, mv, gsm);
-      cta_gemm<double, RECOMP_THREADS>(bk, o.q, kc, -1.0, Bsh, bk, false, Rv + (int64_t)kc * mv, mv, false, 1.0,
-                                       Bsh + (int64_t)kc * bk, bk, gsm);
+    // Bases.  Stacked (rounded_addition, addition.cpp:93-127): Householder QR
+    // of [U_C | U_B] and of [V_C | V_B].  Projected (fast_rounded_addition,
+    // addition.cpp:133-189, the default of fixed-rank plans, and on request
+    // for tolerance plans): U_C and V_C have orthonormal columns (every
+    // target comes from construction, a core SVD / RRQR or the reset
+    // truncation), so U_B is projected out of span(U_C) twice, Zu = U_C^T U_B,
+    // and only the remainder Y_u = U_B - U_C Zu is QR-factored; the same on the
+    // V side.  Both give the same sum C + B = [U_C | Q] M [V_C | Q']^T.
+    const bool proj = (core_method == CORE_FAST ? ws.fixed_rank > 0 : proj_tol != 0) && kc > 0 && o.p > 0 &&
+                      o.q > 0 && !o.left_dense && !o.right_dense && su <= bc && sv <= bk;
+    if (proj) {
+      if (do_u) {
+        cta_project_out<RECOMP_THREADS>(bc, kc, o.p, Ash, bc, Ash + (int64_t)kc * bc, bc, Rc + (int64_t)kc * su, su,
+                                        Xo, gsm);
+        cta_qr_blocked<RECOMP_THREADS>(bc, o.p, Ash + (int64_t)kc * bc, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
+      }
       PHASE_MARK(cls, 1);
-      cta_qr_blocked<RECOMP_THREADS>(bc, o.p, Ash + (int64_t)kc * bc, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
-      cta_qr_blocked<RECOMP_THREADS>(bk, o.q, Bsh + (int64_t)kc * bk, bk, tau_v, Tfv, Wq, smP, smT, gsm, red);
-      PHASE_MARK(cls, 2);
-      // Rc = [I Zu; 0 Ru] (mu x su), Rv = [I Zv; 0 Rv'] (mv x sv)
-      for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
-        const int r = e % mu, c = e / mu;
-        if (c < kc) Rc[e] = (r == c) ? 1.0 : 0.0;
-        else if (r >= kc) Rc[e] = (r - kc <= c - kc) ? Ash[(r - kc) + (int64_t)c * bc] : 0.0;
+      if (do_v) {
+        cta_project_out<RECOMP_THREADS>(bk, kc, o.q, Bsh, bk, Bsh + (int64_t)kc * bk, bk, Rv + (int64_t)kc * sv, sv,
+                                        Yo, gsm);
+        cta_qr_blocked<RECOMP_THREADS>(bk, o.q, Bsh + (int64_t)kc * bk, bk, tau_v, Tfv, side == 1 ? Mtmp : Wq, smP,
+                                       smT, gsm, red);
       }
-      for (int64_t e = threadIdx.x; e < (int64_t)mv * sv; e += blockDim.x) {
-        const int r = e % mv, c = e / mv;
-        if (c < kc) Rv[e] = (r == c) ? 1.0 : 0.0;
-        else if (r >= kc) Rv[e] = (r - kc <= c - kc) ? Bsh[(r - kc) + (int64_t)c * bk] : 0.0;
-      }
-      __syncthreads();
-      // core M (mu x mv) = Rc blockdiag(S_C, T) Rv^T
-      cta_gemm<double, RECOMP_THREADS>(mu, kc, kc, 1.0, Rc, mu, false, Sc, A.kcap, false, 0.0, Mtmp, mu, gsm);
-      cta_gemm<double, RECOMP_THREADS>(mu, o.q, o.p, 1.0, Rc + (int64_t)kc * mu, mu, false, Tm, o.p, false, 0.0,
-                                       Mtmp + (int64_t)kc * mu, mu, gsm);
-      const bool in_smem = (int64_t)mu * mv <= RECOMP_REGION;
-      double* Mm = in_smem ? region : Mg;
-      cta_gemm<double, RECOMP_THREADS>(mu, mv, sv, 1.0, Mtmp, mu, false, Rv, mv, true, 0.0, Mm, mu, gsm);
-      PHASE_MARK(cls, 3);
-      for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) M0[e] = Mm[e];
-      __syncthreads();
-      const int r = svd_core<T, RECOMP_THREADS>(mu, mv, Mm, M0, ws, A.kcap, cnorm, jpvt, Xo, bc, Yo, bk, gsm, &flag, &s_rank);
-      for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
-        const int rr = e % r, c = e / r;
-        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? cnorm[jpvt[c]] : 0.0);
-      }
-      PHASE_MARK(cls, 4);
-      if (threadIdx.x == 0)
-        atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)fast_rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r));
-      // U = [U_C | Q_u] Xo = Q_u [Xo(kc:mu); 0] + U_C Xo(0:kc), through Tm
-      // (bc x r); U_C is read from its FP64 copy in Ash, so Uc is written last
-      for (int side2 = 0; side2 < 2; ++side2) {
-        const int bb = side2 ? bk : bc, pp = side2 ? o.q : o.p;
-        double* X = side2 ? Yo : Xo;
-        double* Bs = side2 ? Bsh : Ash;
-        T* out = side2 ? Vc : Uc;
-        for (int64_t e = threadIdx.x; e < (int64_t)bb * r; e += blockDim.x) {
-          const int rr = e % bb, c = e / bb;
-          Tm[e] = rr < pp ? X[kc + rr + (int64_t)c * bb] : 0.0;
-        }
-        __syncthreads();
-        cta_apply_q_blocked<RECOMP_THREADS>(bb, pp, Bs + (int64_t)kc * bb, bb, side2 ? Tfv : Tfu, r, Tm, (int64_t)bb,
-                                            Wq, smP, smT, gsm, pp);
-        cta_gemm<double, RECOMP_THREADS>(bb, r, kc, 1.0, Bs, bb, false, X, bb, false, 1.0, Tm, bb, gsm);
-        for (int64_t e = threadIdx.x; e < (int64_t)bb * r; e += blockDim.x) {
-          const int rr = e % bb, c = e / bb;
-          out[rr + (int64_t)c * ld] = T(Tm[e]);
-        }
-        __syncthreads();
-      }
-      if (threadIdx.x == 0) A.rank[blk] = r;
-      __syncthreads();
-      PHASE_MARK(cls, 5);
-      continue;
+    } else {
+      if (do_u) cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
+      PHASE_MARK(cls, 1);
+      // the V side of a split target works in Mtmp (free until the core), so
+      // that the two sides never share the W scratch
+      if (do_v) cta_qr_blocked<RECOMP_THREADS>(bk, sv, Bsh, bk, tau_v, Tfv, side == 1 ? Mtmp : Wq, smP, smT, gsm, red);
     }
-    if (do_u) cta_qr_blocked<RECOMP_THREADS>(bc, su, Ash, bc, tau_u, Tfu, Wq, smP, smT, gsm, red);
-    PHASE_MARK(cls, 1);
-    // the V side of a split target works in Mtmp (free until the core), so
-    // that the two sides never share the W scratch
-    if (do_v) cta_qr_blocked<RECOMP_THREADS>(bk, sv, Bsh, bk, tau_v, Tfv, side == 1 ? Mtmp : Wq, smP, smT, gsm, red);
     PHASE_MARK(cls, 2);
     if (side >= 0) {
       // publish this side; the second of the two CTAs goes on with the target
@@ -1199,15 +1146,29 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       if (s_last == 0) continue;
       __threadfence();
     }
-    const int mu = min(bc, su), mv = min(bk, sv);
-    // clean upper-trapezoidal R factors
-    for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
-      const int r = e % mu, c = e / mu;
-      Rc[e] = (r <= c) ? Ash[r + (int64_t)c * bc] : 0.0;
-    }
-    for (int64_t e = threadIdx.x; e < (int64_t)mv * sv; e += blockDim.x) {
-      const int r = e % mv, c = e / mv;
-      Rv[e] = (r <= c) ? Bsh[r + (int64_t)c * bk] : 0.0;
+    const int mu = proj ? su : min(bc, su), mv = proj ? sv : min(bk, sv);
+    if (!proj) {
+      // clean upper-trapezoidal R factors
+      for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
+        const int r = e % mu, c = e / mu;
+        Rc[e] = (r <= c) ? Ash[r + (int64_t)c * bc] : 0.0;
+      }
+      for (int64_t e = threadIdx.x; e < (int64_t)mv * sv; e += blockDim.x) {
+        const int r = e % mv, c = e / mv;
+        Rv[e] = (r <= c) ? Bsh[r + (int64_t)c * bk] : 0.0;
+      }
+    } else {
+      // Rc = [I Zu; 0 Ru] (su x su), Rv = [I Zv; 0 Rv'] (sv x sv); Zu, Zv are in place
+      for (int64_t e = threadIdx.x; e < (int64_t)mu * su; e += blockDim.x) {
+        const int r = e % mu, c = e / mu;
+        if (c < kc) Rc[e] = (r == c) ? 1.0 : 0.0;
+        else if (r >= kc) Rc[e] = (r - kc <= c - kc) ? Ash[(r - kc) + (int64_t)c * bc] : 0.0;
+      }
+      for (int64_t e = threadIdx.x; e < (int64_t)mv * sv; e += blockDim.x) {
+        const int r = e % mv, c = e / mv;
+        if (c < kc) Rv[e] = (r == c) ? 1.0 : 0.0;
+        else if (r >= kc) Rv[e] = (r - kc <= c - kc) ? Bsh[(r - kc) + (int64_t)c * bk] : 0.0;
+      }
     }
     __syncthreads();
     // Mtmp (mu x sv) = [Rc[:, :kc] S_C | Rc[:, kc:] T]
@@ -1307,18 +1268,45 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     }
     PHASE_MARK(cls, 4);
     if (threadIdx.x == 0)
-      atomicAdd(ws.flops + FLOP_RECOMP, (unsigned long long)rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r));
-    // U = Qu Xo ; Vt = Qv Yo  (blocked WY application)
-    // Xo = [Q_core; 0], Yo = [V_core; 0]: rows at or below mu (mv) are zero
-    cta_apply_q_blocked<RECOMP_THREADS>(bc, mu, Ash, bc, Tfu, r, Xo, (int64_t)bc, Wq, smP, smT, gsm, mu);
-    cta_apply_q_blocked<RECOMP_THREADS>(bk, mv, Bsh, bk, Tfv, r, Yo, (int64_t)bk, Wq, smP, smT, gsm, mv);
-    for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
-      const int rr = e % bc, c = e / bc;
-      Uc[rr + (int64_t)c * ld] = T(Xo[e]);
-    }
-    for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
-      const int rr = e % bk, c = e / bk;
-      Vc[rr + (int64_t)c * ld] = T(Yo[e]);
+      atomicAdd(ws.flops + FLOP_RECOMP,
+                (unsigned long long)(proj ? fast_rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r)
+                                          : rounded_addition_flops(bc, bk, bi, kc, o.p, o.q, r)));
+    if (!proj) {
+      // U = Qu Xo ; Vt = Qv Yo  (blocked WY application)
+      // Xo = [Q_core; 0], Yo = [V_core; 0]: rows at or below mu (mv) are zero
+      cta_apply_q_blocked<RECOMP_THREADS>(bc, mu, Ash, bc, Tfu, r, Xo, (int64_t)bc, Wq, smP, smT, gsm, mu);
+      cta_apply_q_blocked<RECOMP_THREADS>(bk, mv, Bsh, bk, Tfv, r, Yo, (int64_t)bk, Wq, smP, smT, gsm, mv);
+      for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
+        const int rr = e % bc, c = e / bc;
+        Uc[rr + (int64_t)c * ld] = T(Xo[e]);
+      }
+      for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
+        const int rr = e % bk, c = e / bk;
+        Vc[rr + (int64_t)c * ld] = T(Yo[e]);
+      }
+    } else {
+      // U = [U_C | Q_u] Xo = Q_u [Xo(kc:mu); 0] + U_C Xo(0:kc), through Tm
+      // (bc x r); U_C is read from its FP64 copy in Ash, so Uc is written last
+      for (int side2 = 0; side2 < 2; ++side2) {
+        const int bb = side2 ? bk : bc, pp = side2 ? o.q : o.p;
+        double* X = side2 ? Yo : Xo;
+        double* Bs = side2 ? Bsh : Ash;
+        T* out = side2 ? Vc : Uc;
+        for (int64_t e = threadIdx.x; e < (int64_t)bb * r; e += blockDim.x) {
+          const int rr = e % bb, c = e / bb;
+          Tm[e] = rr < pp ? X[kc + rr + (int64_t)c * bb] : 0.0;
+        }
+        __syncthreads();
+        cta_apply_q_blocked<RECOMP_THREADS>(bb, pp, Bs + (int64_t)kc * bb, bb, side2 ? Tfv : Tfu, r, Tm, (int64_t)bb,
+                                            Wq, smP, smT, gsm, pp);
+        if (r <= 16) cta_gemm_tall(bb, r, kc, Bs, bb, X, bb, Tm, bb, true);
+        else cta_gemm<double, RECOMP_THREADS>(bb, r, kc, 1.0, Bs, bb, false, X, bb, false, 1.0, Tm, bb, gsm);
+        for (int64_t e = threadIdx.x; e < (int64_t)bb * r; e += blockDim.x) {
+          const int rr = e % bb, c = e / bb;
+          out[rr + (int64_t)c * ld] = T(Tm[e]);
+        }
+        __syncthreads();
+      }
     }
     if (threadIdx.x == 0) A.rank[blk] = r;
     __syncthreads();

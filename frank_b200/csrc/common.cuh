@@ -1005,7 +1005,7 @@ FRANK_D void cta_gemm_tn_dot(int m, int n, int k, double alpha, const TA* A, int
 // thread keeps up to 8 outputs in registers per pass over X's columns.
 template <typename TA, typename TC>
 FRANK_D void cta_gemm_tall(int m, int n, int k, const TA* A, int64_t lda, const double* X, int64_t ldx, TC* C,
-                           int64_t ldc, bool accumulate) {
+                           int64_t ldc, bool accumulate, double alpha = 1.0) {
   for (int c0 = 0; c0 < n; c0 += 8) {
     const int nc = min(8, n - c0);
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
@@ -1018,11 +1018,36 @@ FRANK_D void cta_gemm_tall(int m, int n, int k, const TA* A, int64_t lda, const 
         for (int c = 0; c < 8; ++c)
           if (c < nc) acc[c] += av * X[t + (int64_t)(c0 + c) * ldx];
       }
-      for (int c = 0; c < nc; ++c) {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c >= nc) break;
         TC* pc = C + r + (int64_t)(c0 + c) * ldc;
-        *pc = TC(accumulate ? double(*pc) + acc[c] : acc[c]);
+        *pc = TC(accumulate ? double(*pc) + alpha * acc[c] : alpha * acc[c]);
       }
     }
+  }
+  __syncthreads();
+}
+
+// Project the columns of Y (m x p, ldy) out of the span of Q (m x k, ldq,
+// orthonormal columns), twice (classical Gram-Schmidt with one
+// re-orthogonalisation): Z (k x p, ldz) = Q^T Y_0, Y = (I - Q Q^T)^2 Y_0,
+// Y_0 = Q Z + Y.  Z2 (k x p, ld k) is scratch.  Skinny shapes use the warp /
+// row kernels, larger ones the tiled CTA GEMM.
+template <int NT>
+FRANK_D void cta_project_out(int m, int k, int p, const double* Q, int64_t ldq, double* Y, int64_t ldy, double* Z,
+                             int64_t ldz, double* Z2, double* gsm) {
+  for (int pass = 0; pass < 2; ++pass) {
+    double* Zp = pass ? Z2 : Z;
+    const int64_t ldp = pass ? k : ldz;
+    if ((int64_t)k * p <= 1024) cta_gemm_tn_dot(k, p, m, 1.0, Q, ldq, Y, ldy, Zp, ldp);
+    else cta_gemm<double, NT>(k, p, m, 1.0, Q, ldq, true, Y, ldy, false, 0.0, Zp, ldp, gsm);
+    if (p <= 16) cta_gemm_tall(m, p, k, Q, ldq, Zp, ldp, Y, ldy, true, -1.0);
+    else cta_gemm<double, NT>(m, p, k, -1.0, Q, ldq, false, Zp, ldp, false, 1.0, Y, ldy, gsm);
+  }
+  for (int64_t e = threadIdx.x; e < (int64_t)k * p; e += blockDim.x) {
+    const int r = e % k, c = e / k;
+    Z[r + (int64_t)c * ldz] += Z2[e];
   }
   __syncthreads();
 }
