@@ -215,6 +215,17 @@ class BLRMatrix:
               "frank_blr_refine_device")
         return it.value, res.value
 
+    def autotune(self, force: bool = False, stream: Optional[int] = None) -> dict:
+        """Pick the launch parameters by timing this plan's factorization
+        (frank_blr_autotune); returns them."""
+        check(lib().frank_blr_autotune(self._h, 1 if force else 0, stream), "frank_blr_autotune")
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        v = [C.c_int() for _ in range(3)]
+        check(lib().frank_blr_tuning(self._h, *[C.byref(t) for t in v]), "frank_blr_tuning")
+        return {"band_rows": v[0].value, "split_rank": v[1].value, "projected": bool(v[2].value)}
+
     def write_json(self, path: str, which: int = 0):
         """The block tree with per-block singular values, in the layout of
         FRANK's write_JSON (util/print.cpp:54-128)."""

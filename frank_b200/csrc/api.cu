@@ -9,8 +9,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <random>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -87,6 +89,9 @@ struct frank_blr {
   int core_method = CORE_RRQR;   // core of tolerance plans
   int core_fixed = CORE_FAST;    // core of fixed-rank plans (FRANK_LRA unset: fast_rounded_addition)
   bool proj_tol = false;         // tolerance plans: projected bases (QR of the update's remainder only)
+  // launch parameters the autotuner chooses (frank_blr_autotune)
+  int dupd_band = DUPD_BAND;     // rows per dense-update task
+  int split_p = SPLIT_P;         // split band-1 targets above this operand rank (0: never)
   double core_scale = 0.1;
   int grid_gram = 0;
   double gram_tol = 1e-12;
@@ -300,8 +305,10 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
     const int mm = m * m;
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s, cudaEventRecordExternal));
     {
-      const int nt = (p->bmax + DUPD_TILE - 1) / DUPD_TILE;
-      k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nt * nt, p->grid_dense), DUPD_THREADS, 0, s>>>(W, ws, i);
+      const int band = std::min(p->dupd_band, p->bmax);
+      const int nbands = (p->bmax + band - 1) / band;
+      k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nbands, p->grid_dense), DUPD_THREADS, 0, s>>>(
+          W, ws, i, p->dupd_band);
     }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
     ++launches;
@@ -319,14 +326,14 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
         ++launches;
         if (p->dense_offdiag) {
           k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr, 0);
+              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr, 0, 0);
           ++launches;
         }
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
             W, ws, i, p->smax, p->fixed_rank > 0 ? p->core_fixed : p->core_method, p->core_scale, 0, p->work + i,
             p->rsplit ? p->nsplit : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr,
-            p->proj_tol ? 1 : 0);
+            p->proj_tol ? 1 : 0, p->split_p);
         ++launches;
       }
     }
@@ -1304,6 +1311,125 @@ int frank_blr_write_json(const frank_blr* p, int which, const char* path) {
   const size_t w = fwrite(out.data(), 1, out.size(), f);
   fclose(f);
   if (w != out.size()) return fail(FRANK_ERR_INVALID, std::string("short write to ") + path);
+  return FRANK_OK;
+}
+
+namespace {
+
+// Chosen launch parameters per workload shape, for the life of the process.
+struct TuneKey {
+  int64_t n;
+  int nb, precision, fixed_rank, core_method, lra_fixed;
+  double eps;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(n, nb, precision, fixed_rank, core_method, lra_fixed, eps) <
+           std::tie(o.n, o.nb, o.precision, o.fixed_rank, o.core_method, o.lra_fixed, o.eps);
+  }
+};
+struct TuneVal {
+  int band, split, proj;
+  double ms;
+};
+std::map<TuneKey, TuneVal> g_tuned;
+std::mutex g_tune_mutex;
+
+void drop_graph(frank_blr* p) {
+  if (p->graph_exec) { cudaGraphExecDestroy(p->graph_exec); p->graph_exec = nullptr; }
+  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  p->factored = false;
+}
+
+// Device time (ms) of one factorization with the plan's current parameters:
+// one launch to capture, then the faster of two timed replays.
+int time_factor(frank_blr* p, cudaStream_t s, double* ms) {
+  drop_graph(p);
+  int rc = frank_blr_getrf(p, s);
+  if (rc != FRANK_OK && rc != FRANK_ERR_RANK_OVERFLOW) return rc;
+  cudaEvent_t a = nullptr, b = nullptr;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  double best = 1e300;
+  for (int k = 0; k < 2 && rc == FRANK_OK; ++k) {
+    cudaEventRecord(a, s);
+    rc = frank_blr_getrf(p, s);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    best = std::min(best, (double)t);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return rc == FRANK_ERR_RANK_OVERFLOW ? FRANK_OK : rc;
+}
+
+}  // namespace
+
+int frank_blr_autotune(frank_blr* p, int force, void* stream) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!s) {
+    if (!p->graph_stream) CUDA_TRY(cudaStreamCreateWithFlags(&p->graph_stream, cudaStreamNonBlocking));
+    s = p->graph_stream;
+  }
+  const TuneKey key{p->n, p->nb, p->precision, p->fixed_rank, p->core_method, p->core_fixed, p->eps};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (!force && it != g_tuned.end()) {
+      p->dupd_band = it->second.band;
+      p->split_p = it->second.split;
+      p->proj_tol = it->second.proj != 0;
+      drop_graph(p);
+      return FRANK_OK;
+    }
+  }
+  // coordinate descent over the launch parameters, one at a time, each
+  // candidate timed on the plan's own factorization
+  double best = 0.0;
+  int rc = time_factor(p, s, &best);
+  if (rc) return rc;
+  auto try_values = [&](int* field, std::initializer_list<int> vals) -> int {
+    const int keep = *field;
+    int chosen = keep;
+    for (int v : vals) {
+      if (v == keep) continue;
+      *field = v;
+      double t = 0.0;
+      const int r = time_factor(p, s, &t);
+      if (r) { *field = keep; return r; }
+      if (t < best) { best = t; chosen = v; }
+    }
+    *field = chosen;
+    return FRANK_OK;
+  };
+  if ((rc = try_values(&p->dupd_band, {64, 128, 256}))) return rc;
+  if (p->nlr > 0 && split_on(p) && p->rsplit) {
+    if ((rc = try_values(&p->split_p, {0, 16, 32, 48, 64, 96}))) return rc;
+  }
+  if (p->nlr > 0 && p->fixed_rank == 0 && p->core_method == CORE_RRQR && !p->gram) {
+    int proj = p->proj_tol ? 1 : 0;
+    const int keep = proj;
+    p->proj_tol = !keep;
+    double t = 0.0;
+    if ((rc = time_factor(p, s, &t))) { p->proj_tol = keep; return rc; }
+    if (t < best) { best = t; proj = !keep; }
+    p->proj_tol = proj != 0;
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tuned[key] = TuneVal{p->dupd_band, p->split_p, p->proj_tol ? 1 : 0, best};
+  }
+  drop_graph(p);
+  return FRANK_OK;
+}
+
+int frank_blr_tuning(const frank_blr* p, int* band_rows, int* split_rank, int* projected) {
+  if (!p) return fail(FRANK_ERR_INVALID, "null plan");
+  if (band_rows) *band_rows = p->dupd_band;
+  if (split_rank) *split_rank = p->split_p;
+  if (projected) *projected = p->proj_tol ? 1 : 0;
   return FRANK_OK;
 }
 

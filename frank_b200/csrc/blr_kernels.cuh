@@ -828,52 +828,53 @@ FRANK_D void form_core(const UpdOps<T>& o, int bi, int ld, double* Tm, double* g
 // ---------------------------------------------------------------------------
 // K5: update of dense targets (diagonal blocks and inadmissible blocks):
 // C += XL * T * YR^T  (gemm.cpp:180-200 for LR.LR.D; 126-178 for the others).
-// Persistent grid over the m*m targets of the step, skipping low-rank ones.
+// One task per (target, band of band_rows rows): the band's CTA forms the
+// small core T (p x q) once, X = XL(band, :) T (rows x q) in its scratch slot,
+// and updates its rows of C over the full width, so the core is formed
+// ceil(b / band_rows) times per target and C is streamed in full rows.
 // ---------------------------------------------------------------------------
 constexpr int DUPD_THREADS = 256;
-constexpr int DUPD_TILE = 64;     // output tile of a dense update task
+constexpr int DUPD_BAND = 128;    // rows of a dense update task (default; the autotuner may change it)
 
 template <typename T>
-__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i) {
+__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i, int band_rows) {
   __shared__ double gsm[2 * 16 * 64];
   __shared__ T gsmt[2 * 16 * 64];
   const int m = A.nb - i - 1;
   const int ld = A.bmax;
   const int bi = A.bs(i);
   double* Tm = ws.dscratch + (int64_t)blockIdx.x * ws.dscratch_stride;
+  // X (rn x q, ld ldx) in the second ld x ld half of the slot: ldx * q <= ld * ld
   T* X = reinterpret_cast<T*>(Tm + (int64_t)ld * ld);
-  // tasks: (target, 64 x 64 tile of C); the small core T is recomputed per
-  // tile, so the tiles of one target run on different CTAs
-  const int nt = (ld + DUPD_TILE - 1) / DUPD_TILE, tpb = nt * nt;
-  const int ldx = min(DUPD_TILE, ld);   // X (rn x q) fits the slot's ld x ld region
-  for (int tsk = blockIdx.x; tsk < m * m * tpb; tsk += gridDim.x) {
-    const int pair = tsk / tpb, tile = tsk % tpb;
+  const int bandr = min(band_rows, ld);
+  const int ldx = bandr;
+  const int nbands = (ld + bandr - 1) / bandr;
+  for (int tsk = blockIdx.x; tsk < m * m * nbands; tsk += gridDim.x) {
+    const int pair = tsk / nbands, band = tsk % nbands;
     const int ic = i + 1 + pair / m, k = i + 1 + pair % m;
     if (A.is_lr(ic, k)) continue;
     const int bc = A.bs(ic), bk = A.bs(k);
-    const int r0 = (tile / nt) * DUPD_TILE, c0 = (tile % nt) * DUPD_TILE;
-    if (r0 >= bc || c0 >= bk) continue;
-    const int rn = min(DUPD_TILE, bc - r0), cn = min(DUPD_TILE, bk - c0);
-    T* C = A.dense(ic, k) + r0 + (int64_t)c0 * ld;
+    const int r0 = band * bandr;
+    if (r0 >= bc) continue;
+    const int rn = min(bandr, bc - r0);
+    T* C = A.dense(ic, k) + r0;
     UpdOps<T> o = update_operands(A, ws, i, ic, k);
-    if (threadIdx.x == 0 && tile == 0)
+    if (threadIdx.x == 0 && band == 0)
       atomicAdd(ws.flops + FLOP_DENSE, (unsigned long long)(2.0 * bc * bk * o.q + 2.0 * bc * o.p * o.q +
                                                             2.0 * bi * o.p * o.q));
     if (o.left_dense && o.right_dense) {
       // C -= A(ic,i) A(i,k)
-      cta_gemm<T, DUPD_THREADS>(rn, cn, bi, T(-1), o.XL + r0, ld, false, o.YR + (int64_t)c0 * ld, ld, false, T(1), C,
-                                ld, gsmt);
+      cta_gemm<T, DUPD_THREADS>(rn, bk, bi, T(-1), o.XL + r0, ld, false, o.YR, ld, false, T(1), C, ld, gsmt);
       continue;
     }
     form_core<T, DUPD_THREADS>(o, bi, ld, Tm, gsm);
     // X = XL(r0 : r0+rn, :) T  (rn x q), accumulate in the working precision
     cta_gemm<T, DUPD_THREADS>(rn, o.q, o.p, T(1), o.XL + r0, ld, false, Tm, o.p, false, T(0), X, ldx, gsmt);
-    // C(tile) += X * YR(c0 : c0+cn, :)^T
+    // C(band) += X * YR^T
     if (!o.right_dense)
-      cta_gemm<T, DUPD_THREADS>(rn, cn, o.q, T(1), X, ldx, false, o.YR + c0, ld, true, T(1), C, ld, gsmt);
+      cta_gemm<T, DUPD_THREADS>(rn, bk, o.q, T(1), X, ldx, false, o.YR, ld, true, T(1), C, ld, gsmt);
     else
-      cta_gemm<T, DUPD_THREADS>(rn, cn, o.q, T(1), X, ldx, false, o.YR + (int64_t)c0 * ld, ld, false, T(1), C,
-                                ld, gsmt);
+      cta_gemm<T, DUPD_THREADS>(rn, bk, o.q, T(1), X, ldx, false, o.YR, ld, false, T(1), C, ld, gsmt);
   }
 }
 
@@ -896,7 +897,7 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
 // The core lives in shared memory when it fits (RECOMP_SMEM_CORE doubles).
 // ---------------------------------------------------------------------------
 constexpr int RECOMP_THREADS = 512;
-constexpr int SPLIT_P = 32;       // split band-1 targets whose operand rank exceeds this
+constexpr int SPLIT_P = 32;       // split band-1 targets whose operand rank exceeds this (default)
 constexpr int SPLIT_MAX = 128;    // band-1 tasks eligible for the split (scratch slots)
 constexpr int RECOMP_SMEM_BYTES = 227 * 1024 - 512;     // dynamic shared memory (all but the static part)
 constexpr int RECOMP_GSM = 2 * 16 * 64;                 // cta_gemm tiles (doubles)
@@ -1020,7 +1021,8 @@ template <typename T>
 __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
                                                                int core_method, double core_scale,
                                                                int only_dense_operands, int* counter, int nsplit,
-                                                               double* split_base, int* split_done, int proj_tol) {
+                                                               double* split_base, int* split_done, int proj_tol,
+                                                               int split_p) {
   extern __shared__ double dsm[];
   double* gsm = dsm;
   double* region = dsm + RECOMP_GSM;
@@ -1063,8 +1065,8 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     const int ic = i + 1 + a_, k = i + 1 + c_;
     if (!A.is_lr(ic, k)) continue;
     if (only_dense_operands && A.is_lr(ic, i) && A.is_lr(i, k)) continue;
-    const bool split_t = tsk < nspl && A.is_lr(ic, i) && A.is_lr(i, k) &&
-                         max(A.rank[ic * A.nb + i], A.rank[i * A.nb + k]) > SPLIT_P;
+    const bool split_t = tsk < nspl && split_p > 0 && A.is_lr(ic, i) && A.is_lr(i, k) &&
+                         max(A.rank[ic * A.nb + i], A.rank[i * A.nb + k]) > split_p;
     if ((side >= 0) != split_t) continue;
     set_base(side >= 0 ? split_base + (int64_t)tsk * ws.rscratch_stride : cta_base);
     const bool do_u = side != 1, do_v = side != 0;

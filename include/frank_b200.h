@@ -271,6 +271,20 @@ int frank_batch_refine_device(frank_batch* batch, const double* const* d_b, int6
  * (util/print.cpp:124-128). */
 int frank_blr_write_json(const frank_blr* plan, int which, const char* path);
 
+/* Autotuner of the plan's launch parameters: the rows per dense-update task
+ * (64 / 128 / 256), the operand rank above which a band-1 recompression
+ * target is split over two CTAs (never / 16 ... 96), and, for tolerance plans
+ * with the RRQR core, stacked or projected bases.  Coordinate descent, one
+ * parameter at a time, each candidate timed on the plan's own factorization
+ * (device time of a captured-graph replay); the choice is cached for the
+ * process per workload shape (n, nb, precision, rank / tolerance,
+ * recompression) and reused by later calls unless `force`.  Leaves the plan
+ * unfactored.  No reference counterpart. */
+int frank_blr_autotune(frank_blr* plan, int force, void* stream);
+
+/* The plan's current launch parameters (see frank_blr_autotune). */
+int frank_blr_tuning(const frank_blr* plan, int* band_rows, int* split_rank, int* projected);
+
 /* Counters of the last getrf: kernels launched by it plus those of every
  * solve / matvec / refine since, recompressions performed, the largest
  * recompressed rank and the number of ranks clamped at max_rank. */
