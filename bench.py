@@ -523,18 +523,26 @@ RECOMP_TRAFFIC = None
 
 def profile_case(name):
     """Small single-GPU cases for ncu captures (`--profile-case`): build the
-    plan, run one getrf, print the per-class kernel times.
-      n8192: Laplace-3D N=8192, 16 x 16 blocks of 512, A_H eps 1e-8, mixed
-             factor at 1e-6 (the recompression profile case)."""
+    plan, run the factorization, print the per-class kernel times.
+      n8192:       Laplace-3D N=8192 (the headline point stream), 16 x 16
+                   blocks of 512, A_H eps 1e-8, mixed factor at the
+                   headline's tolerance (the recompression profile case);
+      n8192-solve: the same plan, then one 4-RHS solve and one H-matvec
+                   (the solve / matvec profile case)."""
     import torch
     from frank_b200 import BLRMatrix
-    if name != "n8192":
+    if name not in ("n8192", "n8192-solve"):
         raise SystemExit("unknown profile case " + name)
-    x = make_points(8192, 3, 2, 10)
-    M = BLRMatrix(8192, 16, eps=1e-6, precision="mixed")
-    M.build_kernel("laplace", x, 1e-8)
+    x = make_points(8192, 3, CFG["point_seed"], CFG["morton_level"])
+    M = BLRMatrix(8192, 16, eps=CFG["mixed_eps"], precision="mixed")
+    M.build_kernel("laplace", x, CFG["eps"])
     M.set_timing(True)
     M.getrf()
+    if name == "n8192-solve":
+        b = torch.from_numpy(make_rhs(8192, CFG["nrhs"], CFG["rhs_seed"]).T.copy()).cuda()
+        y = torch.zeros_like(b)
+        M.solve_device(b.data_ptr(), CFG["nrhs"])
+        M.matvec_device(b.data_ptr(), y.data_ptr(), CFG["nrhs"])
     torch.cuda.synchronize()
     print(json.dumps(M.kernel_times()))
     M.close()

@@ -221,6 +221,10 @@ class BLRMatrix:
         check(lib().frank_blr_autotune(self._h, 1 if force else 0, stream), "frank_blr_autotune")
         return self.tuning()
 
+    def set_tuning(self, band_rows: int = 128, split_rank: int = 32, projected: bool = False):
+        check(lib().frank_blr_set_tuning(self._h, int(band_rows), int(split_rank), 1 if projected else 0),
+              "frank_blr_set_tuning")
+
     def tuning(self) -> dict:
         v = [C.c_int() for _ in range(3)]
         check(lib().frank_blr_tuning(self._h, *[C.byref(t) for t in v]), "frank_blr_tuning")

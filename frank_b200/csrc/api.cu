@@ -138,7 +138,7 @@ struct frank_blr {
   // lookahead: second capture stream and its dependency events
   cudaStream_t aux = nullptr;
   cudaEvent_t fork = nullptr;
-  std::vector<cudaEvent_t> getrf_done, dense_done;
+  std::vector<cudaEvent_t> getrf_done, dense_done, panel_done;
 };
 
 namespace {
@@ -196,7 +196,10 @@ bool pretruncate(const frank_blr* p) {
          p->rstride >= 4 * (int64_t)p->kcap * p->kcap + 8 * (int64_t)p->kcap;
 }
 
-cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * FLOP_SLOTS + cls) * 2 + end]; }
+// timing events per step: one pair per operation class, plus one for the
+// update of the next diagonal block (counted with the dense class)
+constexpr int EV_DENSE_NEXT = FLOP_SLOTS, EV_SLOTS = FLOP_SLOTS + 1;
+cudaEvent_t& ev_at(frank_blr* p, int step, int cls, int end) { return p->ev[((size_t)step * EV_SLOTS + cls) * 2 + end]; }
 
 // Split recompression targets (two CTAs per large band-1 target) on plans
 // with the full recompression grid (not the reduced grids of batched plans).
@@ -225,11 +228,13 @@ int ensure_scratch(frank_blr* p) {
   return FRANK_OK;
 }
 
-// One factorization on stream s.  The leaf getrf of step i+1 runs on a second
-// stream (p->aux) as soon as step i's dense-target update has refreshed the
-// diagonal block (i+1, i+1), so it overlaps step i's recompressions
-// (lookahead of depth one); the panel of step i+1 waits for both.  The
-// recompression grid leaves one SM free for it.
+// One factorization on stream s.  After step i's panels, a second stream
+// (p->aux) updates the diagonal block (i+1, i+1), runs the leaf getrf of
+// step i+1 and then updates the step's other dense targets, all overlapping
+// step i's recompressions on s (lookahead of depth one); the main stream
+// waits for the dense updates before the next panels, and for the getrf
+// before the next inverses.  The recompression grid leaves one SM free for
+// the second stream.
 template <typename T>
 int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   p->timed = timing;
@@ -278,7 +283,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   };
   int rc = getrf_on_aux(0);
   if (rc) return rc;
-  ++launches;
+  ++launches;   // the getrf load kernel
   for (int i = 0; i < p->nb; ++i) {
     CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[i], 0));
     {
@@ -303,19 +308,31 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 1), s, cudaEventRecordExternal));
     ++launches;
     const int mm = m * m;
-    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s, cudaEventRecordExternal));
+    // Dense targets on the second stream, concurrently with the
+    // recompressions (the two write disjoint blocks and read the same
+    // panels): the next diagonal block first, its leaf getrf, then the other
+    // dense targets.  The next panel overwrites WL / WU, so the main stream
+    // waits for all of it after the recompressions.
+    CUDA_TRY(cudaEventRecord(p->panel_done[i], s));
+    CUDA_TRY(cudaStreamWaitEvent(s2, p->panel_done[i], 0));
     {
       const int band = std::min(p->dupd_band, p->bmax);
       const int nbands = (p->bmax + band - 1) / band;
-      k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nbands, p->grid_dense), DUPD_THREADS, 0, s>>>(
-          W, ws, i, p->dupd_band);
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 0), s2, cudaEventRecordExternal));
+      k_update_dense<T><<<nbands, DUPD_THREADS, 0, s2>>>(W, ws, i, p->dupd_band, DUPD_NEXT);
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 1), s2, cudaEventRecordExternal));
+      ++launches;
+      if ((rc = getrf_on_aux(i + 1))) return rc;
+      ++launches;   // the getrf load kernel
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s2, cudaEventRecordExternal));
+      if (m > 1) {
+        k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nbands, p->grid_dense), DUPD_THREADS, 0, s2>>>(
+            W, ws, i, p->dupd_band, DUPD_REST);
+        ++launches;
+      }
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s2, cudaEventRecordExternal));
+      CUDA_TRY(cudaEventRecord(p->dense_done[i], s2));
     }
-    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s, cudaEventRecordExternal));
-    ++launches;
-    CUDA_TRY(cudaEventRecord(p->dense_done[i], s));
-    CUDA_TRY(cudaStreamWaitEvent(s2, p->dense_done[i], 0));
-    if ((rc = getrf_on_aux(i + 1))) return rc;
-    ++launches;
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 0), s, cudaEventRecordExternal));
     if (p->nlr > 0) {
       if (use_gram(p)) {
@@ -338,6 +355,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
       }
     }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 1), s, cudaEventRecordExternal));
+    CUDA_TRY(cudaStreamWaitEvent(s, p->dense_done[i], 0));
   }
   CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[p->nb - 1], 0));
   CUDA_TRY(cudaGetLastError());
@@ -350,12 +368,12 @@ int collect_times(frank_blr* p) {
   for (int c = 0; c < FLOP_SLOTS; ++c) p->class_ms[c] = 0.0;
   if (!p->timed) return FRANK_OK;
   for (int i = 0; i < p->nb; ++i)
-    for (int c = 0; c < FLOP_SLOTS; ++c) {
+    for (int c = 0; c < EV_SLOTS; ++c) {
       if (i == p->nb - 1 && c != FLOP_GETRF && c != FLOP_TRINV) continue;
       float ms = 0.f;
       cudaError_t e = cudaEventElapsedTime(&ms, ev_at(p, i, c, 0), ev_at(p, i, c, 1));
       if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("event timing: ") + cudaGetErrorString(e));
-      p->class_ms[c] += ms;
+      p->class_ms[c == EV_DENSE_NEXT ? FLOP_DENSE : c] += ms;
     }
   return FRANK_OK;
 }
@@ -588,6 +606,7 @@ void free_plan(frank_blr* p) {
   for (cudaEvent_t e : p->ev) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : p->getrf_done) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : p->dense_done) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->panel_done) if (e) cudaEventDestroy(e);
   if (p->fork) cudaEventDestroy(p->fork);
   if (p->aux) cudaStreamDestroy(p->aux);
   if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
@@ -768,12 +787,13 @@ int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_bl
     free_plan(p);
     return fail(FRANK_ERR_CUDA, "cudaMallocHost");
   }
-  p->ev.assign((size_t)nb * FLOP_SLOTS * 2, nullptr);
+  p->ev.assign((size_t)nb * EV_SLOTS * 2, nullptr);
   for (auto& e : p->ev)
     if (cudaEventCreate(&e) != cudaSuccess) { free_plan(p); return fail(FRANK_ERR_CUDA, "cudaEventCreate"); }
   p->getrf_done.assign(nb, nullptr);
   p->dense_done.assign(nb, nullptr);
-  for (auto* v : {&p->getrf_done, &p->dense_done})
+  p->panel_done.assign(nb, nullptr);
+  for (auto* v : {&p->getrf_done, &p->dense_done, &p->panel_done})
     for (auto& e : *v)
       if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
         free_plan(p);
@@ -1421,6 +1441,15 @@ int frank_blr_autotune(frank_blr* p, int force, void* stream) {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     g_tuned[key] = TuneVal{p->dupd_band, p->split_p, p->proj_tol ? 1 : 0, best};
   }
+  drop_graph(p);
+  return FRANK_OK;
+}
+
+int frank_blr_set_tuning(frank_blr* p, int band_rows, int split_rank, int projected) {
+  if (!p || band_rows < 16 || split_rank < 0) return fail(FRANK_ERR_INVALID, "bad tuning values");
+  p->dupd_band = band_rows;
+  p->split_p = split_rank;
+  p->proj_tol = projected != 0;
   drop_graph(p);
   return FRANK_OK;
 }

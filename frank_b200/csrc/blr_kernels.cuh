@@ -832,12 +832,16 @@ FRANK_D void form_core(const UpdOps<T>& o, int bi, int ld, double* Tm, double* g
 // small core T (p x q) once, X = XL(band, :) T (rows x q) in its scratch slot,
 // and updates its rows of C over the full width, so the core is formed
 // ceil(b / band_rows) times per target and C is streamed in full rows.
+// Modes: every dense target of the step, only the next diagonal block
+// (i+1, i+1) (which the next leaf getrf waits for), or all but that block.
 // ---------------------------------------------------------------------------
 constexpr int DUPD_THREADS = 256;
 constexpr int DUPD_BAND = 128;    // rows of a dense update task (default; the autotuner may change it)
+enum DenseUpdateMode { DUPD_ALL = 0, DUPD_NEXT = 1, DUPD_REST = 2 };
 
 template <typename T>
-__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i, int band_rows) {
+__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i, int band_rows,
+                                                                int mode) {
   __shared__ double gsm[2 * 16 * 64];
   __shared__ T gsmt[2 * 16 * 64];
   const int m = A.nb - i - 1;
@@ -849,8 +853,11 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
   const int bandr = min(band_rows, ld);
   const int ldx = bandr;
   const int nbands = (ld + bandr - 1) / bandr;
-  for (int tsk = blockIdx.x; tsk < m * m * nbands; tsk += gridDim.x) {
+  // pair 0 is the next diagonal block (i+1, i+1)
+  const int ntask = mode == DUPD_NEXT ? nbands : m * m * nbands;
+  for (int tsk = blockIdx.x; tsk < ntask; tsk += gridDim.x) {
     const int pair = tsk / nbands, band = tsk % nbands;
+    if (mode == DUPD_REST && pair == 0) continue;
     const int ic = i + 1 + pair / m, k = i + 1 + pair % m;
     if (A.is_lr(ic, k)) continue;
     const int bc = A.bs(ic), bk = A.bs(k);
@@ -909,53 +916,85 @@ constexpr int RECOMP_REGION = RECOMP_SMEM_BYTES / 8 - RECOMP_GSM;  // doubles fo
 // only the remainders are QR-factored; SVD core as above).
 enum CoreMethod { CORE_RRQR = 0, CORE_SVD = 1, CORE_FAST = 2 };
 
-// SVD of the recompression core Mm (mu x mv, ld mu; M0 holds a copy) by
-// one-sided Jacobi, in place.  Rank: the fixed rank of the plan, else
-// find_svd_truncation_rank (misc.cpp:133-146, quirk included) at ws.eps;
-// capped at kcap (counted as a rank overflow).  On return sig[ord[c]] is the
-// c-th largest singular value, Xo (bc x r, ld bc) = [U_m(:, :r); 0] and Yo
-// (bk x r, ld bk) = [V_m(:, :r); 0].  Returns r (all threads).
+// SVD of the recompression core Mm (mu x mv, ld mu), preconditioned
+// one-sided Jacobi: column-pivoted QR M P = Q R (in place in Mm), then
+// one-sided Jacobi on the columns of A = R^T (mv x k) with the rotations
+// accumulated in Z (k x k, appended rows); the pivoting leaves A's columns
+// nearly orthogonal, so a few sweeps converge (Drmac & Veselic, "New fast and
+// accurate Jacobi SVD algorithm", SIAM J. Matrix Anal. Appl. 29, 2008).
+// With A Z = W S: M = (Q Z) S (P W)^T, so the left singular vectors are Q Z
+// (the QR's reflectors applied to Z) and the right ones P W (the normalised
+// columns of A Z, rows permuted back); both sets are orthonormal to working
+// accuracy whatever the singular value, which the next projected addition
+// into this target relies on.  Tolerance plans stop the QR once the
+// remaining columns are below thr = 0.01 eps ||M||_F / sqrt(mv min(mu, mv)),
+// so the dropped block R22 moves the truncation test below by at most 1 % of
+// its threshold.  Rank: the fixed rank of the plan, else
+// find_svd_truncation_rank (misc.cpp:133-146, quirk included: the tail error
+// is (min_dim - r) sigma_r^2) at ws.eps with ||M||_F as the reference norm;
+// capped at kcap (counted as a rank overflow).  Scratch: the Jacobi matrix
+// ((mv + k) x k) in smem (region, cap doubles, after the core if the core is
+// there) when it fits, else in Atmp (global, (mv + min(mu,mv)) x min(mu,mv));
+// tau / cnorm / partial / jpvt (mv each), sig / ord (min(mu, mv)).  On return
+// partial[c] is the c-th largest singular value (c < r), Xo (bc x r, ld bc) =
+// [U_m(:, :r); 0] and Yo (bk x r, ld bk) = [V_m(:, :r); 0].  Returns r (all
+// threads).
 template <typename T, int NT>
-FRANK_D int svd_core(int mu, int mv, double* Mm, const double* M0, const FactorWs<T>& ws, int kcap, double* sig,
-                     int* ord, double* Xo, int bc, double* Yo, int bk, double* gsm, int* flag, int* s_rank) {
-  const int sweeps = cta_jacobi_columns(mu, mv, Mm, mu, 60, flag);
+FRANK_D int svd_core(int mu, int mv, double* Mm, const FactorWs<T>& ws, int kcap, double* region, int64_t cap,
+                     double* Atmp, double* tau, double* cnorm, double* partial, int* jpvt, double* sig, int* ord,
+                     double* Xo, int bc, double* Yo, int bk, double* red, int* redi, int* flag, int* s_rank) {
+  const int nsv = min(mu, mv);
+  double f = 0.0;
+  for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) f += Mm[e] * Mm[e];
+  const double fro = sqrt(block_sum(f, red));
+  const double thr = ws.fixed_rank > 0 ? 0.0 : 0.01 * ws.eps * fro / sqrt((double)mv * (double)nsv);
+  const int k = cta_truncated_geqp3(mu, mv, Mm, mu, thr, nsv, tau, cnorm, partial, jpvt, red, redi);
+  // [A; I] with A = R(0:k, :)^T (mv x k), ld mv + k
+  const int ldj = mv + k;
+  const int64_t off = (Mm == region) ? (int64_t)mu * mv : 0;
+  double* Aj = off + (int64_t)ldj * k <= cap ? region + off : Atmp;
+  for (int64_t e = threadIdx.x; e < (int64_t)ldj * k; e += blockDim.x) {
+    const int c = e % ldj, j = e / ldj;
+    Aj[e] = c < mv ? ((c >= j) ? Mm[j + (int64_t)c * mu] : 0.0) : (c - mv == j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const int sweeps = cta_jacobi_columns(mv, k, Aj, ldj, 60, flag, ldj);
   if (sweeps < 0 && threadIdx.x == 0) atomicAdd(ws.err + ERR_JACOBI, 1);
-  for (int c = threadIdx.x >> 5; c < mv; c += blockDim.x >> 5) {
+  for (int c = threadIdx.x >> 5; c < k; c += blockDim.x >> 5) {
     double sacc = 0.0;
-    for (int rr = threadIdx.x & 31; rr < mu; rr += 32) sacc += Mm[rr + (int64_t)c * mu] * Mm[rr + (int64_t)c * mu];
+    for (int rr = threadIdx.x & 31; rr < mv; rr += 32) sacc += Aj[rr + (int64_t)c * ldj] * Aj[rr + (int64_t)c * ldj];
     sacc = warp_sum(sacc);
     if ((threadIdx.x & 31) == 0) sig[c] = sqrt(sacc);
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < mv; c += blockDim.x) {
+  for (int c = threadIdx.x; c < k; c += blockDim.x) {
     const double v = sig[c];
     int pos = 0;
-    for (int d = 0; d < mv; ++d) {
+    for (int d = 0; d < k; ++d) {
       const double w = sig[d];
       pos += (w > v) || (w == v && d < c);
     }
     ord[pos] = c;
   }
   __syncthreads();
-  const int nsv = min(mu, mv);
   if (threadIdx.x == 0) {
     int rr;
     if (ws.fixed_rank > 0) {
       rr = min(ws.fixed_rank, nsv);
     } else {
-      double fro = 0.0;
-      for (int j = 0; j < nsv; ++j) { const double v = sig[ord[j]]; fro += v * v; }
-      const double thr = ws.eps * sqrt(fro);
+      // singular values beyond the k computed ones are below ||R22||, which
+      // satisfies the test by the choice of thr: count them as zero
+      const double thr_t = ws.eps * fro;
       rr = 0;
       double err;
       do {
         ++rr;
         err = 0.0;
         if (rr < nsv) {
-          const double v = sig[ord[rr]];
-          for (int j = rr; j < nsv; ++j) err += v * v;
+          const double v = rr < k ? sig[ord[rr]] : 0.0;
+          err = (double)(nsv - rr) * v * v;
         }
-      } while (rr < nsv && sqrt(err) > thr);
+      } while (rr < nsv && sqrt(err) > thr_t);
     }
     if (rr > kcap) { atomicAdd(ws.err + ERR_RANK_OVERFLOW, 1); rr = kcap; }
     atomicMax(ws.err + ERR_MAX_RANK, rr);
@@ -964,20 +1003,24 @@ FRANK_D int svd_core(int mu, int mv, double* Mm, const double* M0, const FactorW
   }
   __syncthreads();
   const int r = *s_rank;
+  // Yo (bk x r): V_M = P W, row jpvt[i] of V_M = row i of W (columns of A Z
+  // normalised); Xo (bc x r) = [Z(:, ord); 0], then Q applied below
+  for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) Yo[e] = 0.0;
   for (int64_t e = threadIdx.x; e < (int64_t)bc * r; e += blockDim.x) {
-    const int rr = e % bc, c = e / bc;
-    const int src = ord[c];
-    const double sv_ = sig[src];
-    Xo[e] = (rr < mu && sv_ > 0.0) ? Mm[rr + (int64_t)src * mu] / sv_ : 0.0;
+    const int i = e % bc, c = e / bc;
+    Xo[e] = (i < k && c < k) ? Aj[mv + i + (int64_t)ord[c] * ldj] : 0.0;
   }
   __syncthreads();
-  // Yo (bk x r): rows < mv = M0^T Um / sigma
-  cta_gemm<double, NT>(mv, r, mu, 1.0, M0, mu, true, Xo, bc, false, 0.0, Yo, bk, gsm);
-  for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
-    const int rr = e % bk, c = e / bk;
-    const double sv_ = sig[ord[c]];
-    Yo[e] = (rr < mv && sv_ > 0.0) ? Yo[e] / sv_ : 0.0;
+  for (int64_t e = threadIdx.x; e < (int64_t)mv * r; e += blockDim.x) {
+    const int i = e % mv, c = e / mv;
+    const int src = c < k ? ord[c] : -1;
+    const double sv_ = src >= 0 ? sig[src] : 0.0;
+    Yo[jpvt[i] + (int64_t)c * bk] = sv_ > 0.0 ? Aj[i + (int64_t)src * ldj] / sv_ : 0.0;
   }
+  __syncthreads();
+  cta_apply_q(mu, k, Mm, mu, tau, r, Xo, (int64_t)bc);
+  // the kept singular values in order, in partial (free after the QR)
+  for (int c = threadIdx.x; c < r; c += blockDim.x) partial[c] = c < k ? sig[ord[c]] : 0.0;
   __syncthreads();
   return r;
 }
@@ -1258,13 +1301,12 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       }
       __syncthreads();
     } else {
-      // SVD core: keep a copy for the V side, Jacobi in place
-      for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) M0[e] = Mm[e];
-      __syncthreads();
-      r = svd_core<T, RECOMP_THREADS>(mu, mv, Mm, M0, ws, A.kcap, cnorm, jpvt, Xo, bc, Yo, bk, gsm, &flag, &s_rank);
+      // SVD core (Rc / Rv are free once the core is formed: Jacobi scratch)
+      r = svd_core<T, RECOMP_THREADS>(mu, mv, Mm, ws, A.kcap, region, RECOMP_REGION, Rc, tau_c, cnorm, pnorm, jpvt,
+                                      tau2, jinv, Xo, bc, Yo, bk, red, redi, &flag, &s_rank);
       for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
         const int rr = e % r, c = e / r;
-        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? cnorm[jpvt[c]] : 0.0);
+        Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? pnorm[c] : 0.0);
       }
       __syncthreads();
     }

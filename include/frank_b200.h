@@ -282,6 +282,10 @@ int frank_blr_write_json(const frank_blr* plan, int which, const char* path);
  * unfactored.  No reference counterpart. */
 int frank_blr_autotune(frank_blr* plan, int force, void* stream);
 
+/* Set the launch parameters by hand (band_rows >= 16; split_rank 0 = never
+ * split; projected: bases of tolerance plans with the RRQR core). */
+int frank_blr_set_tuning(frank_blr* plan, int band_rows, int split_rank, int projected);
+
 /* The plan's current launch parameters (see frank_blr_autotune). */
 int frank_blr_tuning(const frank_blr* plan, int* band_rows, int* split_rank, int* projected);
 

@@ -962,7 +962,8 @@ def geqp3(A: np.ndarray):
     columns free); returns R (the upper triangle of the factored matrix,
     n x n) and the 0-based column order."""
     m, n = A.shape
-    qr_, jpvt, tau, work, info = lapack.dgeqp3(np.asfortranarray(A.copy()), np.zeros(n, dtype=np.int32))
+    # scipy's wrapper starts from jpvt = 0 (every column free), as the reference does
+    qr_, jpvt, tau, work, info = lapack.dgeqp3(np.asfortranarray(A.copy()))
     R = np.zeros((n, n))
     k = min(m, n)
     R[:k, :] = np.triu(qr_[:k, :])
