@@ -309,6 +309,10 @@ def run_ours(args, rank, world):
                             ("fp64_at_mixed_eps", "fp64", c["mixed_eps"])):
         M = BLRMatrix(c["n"], c["nb"], eps=feps, precision=prec)
         M.build_kernel(c["kernel"], x, c["eps"])
+        # launch parameters by the plan's own autotuner (a few timed
+        # factorizations, before the warm-up); the FP64 arm at 1e-8 keeps the
+        # defaults, its factorizations being too long to tune within minutes
+        tuning = M.autotune(stream=stream) if arm != "fp64" else M.tuning()
         torch.cuda.synchronize()
 
         def step():
@@ -373,7 +377,7 @@ def run_ours(args, rank, world):
         matvec_ms = ev(lambda: M.matvec_device(b_dev.data_ptr(), y.data_ptr(), c["nrhs"], stream=stream))
         elem = 8 if prec == "fp64" else 4
         ranks = [M.rank(i, j, 1) for i in range(c["nb"]) for j in range(c["nb"]) if i != j]
-        arms[arm] = dict(times=times, its=its, res=ress, kt=kt, e2e=e2e, clocks=clocks, stats=st,
+        arms[arm] = dict(times=times, its=its, res=ress, kt=kt, e2e=e2e, clocks=clocks, stats=st, tuning=tuning,
                          mean_rank=float(np.mean(ranks)), max_rank=int(max(ranks)), prec=prec, factor_eps=feps,
                          solve_ms=solve_ms, matvec_ms=matvec_ms, solve_bytes=plan_bytes(M, 1, elem),
                          matvec_bytes=plan_bytes(M, 0, 8))
@@ -513,12 +517,14 @@ def run_ours_sample(stream, steps):
     return out
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one
-# k_recompress launch measured by ncu on the profile case (`--profile-case
-# n8192`, the mixed factor at the headline's tolerance), in bytes, and the
-# same launch's algorithmic FLOPs: the per-launch figures behind the roofline
-# (profiles/k_recompress_blr_laplace3d_n8192.md).  None until captured.
-RECOMP_TRAFFIC = None
+# DRAM traffic of k_recompress per algorithmic FLOP, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over all 15 recompression
+# launches of `--profile-case n8192`, the mixed factor at the headline's
+# tolerance: 1.610e9 bytes for 5.454e10 FLOPs; the workload is too large to
+# capture whole).  The roofline's `traffic` scales it to the mean headline
+# launch by the FLOPs that launch performs
+# (profiles/k_recompress_blr_laplace3d_n8192.md).
+RECOMP_BYTES_PER_FLOP = 1.610e9 / 5.454e10
 
 
 def profile_case(name):
@@ -528,11 +534,26 @@ def profile_case(name):
                    blocks of 512, A_H eps 1e-8, mixed factor at the
                    headline's tolerance (the recompression profile case);
       n8192-solve: the same plan, then one 4-RHS solve and one H-matvec
-                   (the solve / matvec profile case)."""
+                   (the solve / matvec profile case);
+      headline:    the benchmark's workload (N=32768, 64 x 64 blocks of 512),
+                   one mixed factorization and one refinement to 1e-10, no
+                   timing events (the launch list of one step)."""
     import torch
     from frank_b200 import BLRMatrix
-    if name not in ("n8192", "n8192-solve"):
+    if name not in ("n8192", "n8192-solve", "headline"):
         raise SystemExit("unknown profile case " + name)
+    if name == "headline":
+        x = make_points(CFG["n"], CFG["dim"], CFG["point_seed"], CFG["morton_level"])
+        M = BLRMatrix(CFG["n"], CFG["nb"], eps=CFG["mixed_eps"], precision="mixed")
+        M.build_kernel("laplace", x, CFG["eps"])
+        b = torch.from_numpy(make_rhs(CFG["n"], CFG["nrhs"], CFG["rhs_seed"]).T.copy()).cuda()
+        xd = torch.zeros_like(b)
+        M.getrf()
+        it, res = M.refine_device(b.data_ptr(), xd.data_ptr(), CFG["nrhs"], tol=CFG["tol"], maxit=60)
+        torch.cuda.synchronize()
+        print(json.dumps({"refine_iters": it, "residual": res, "stats": M.stats()}))
+        M.close()
+        return
     x = make_points(8192, 3, CFG["point_seed"], CFG["morton_level"])
     M = BLRMatrix(8192, 16, eps=CFG["mixed_eps"], precision="mixed")
     M.build_kernel("laplace", x, CFG["eps"])
@@ -696,10 +717,10 @@ def main():
             "fp64": {"value": t_fp64, "unit": "s", "iters": fp["its"][-1], "residual": fp["res"][-1],
                      "mean_rank": fp["mean_rank"], "max_rank": fp["max_rank"], "kernel_ms": fp["kt"][-1]},
             "mixed": {"iters": mx["its"][-1], "residual": mx["res"][-1], "mean_rank": mx["mean_rank"],
-                      "max_rank": mx["max_rank"], "kernel_ms": kt},
+                      "max_rank": mx["max_rank"], "kernel_ms": kt, "tuning": mx["tuning"]},
             "fp64_at_mixed_eps": {"value": t_ctl, "unit": "s", "factor_eps": CFG["mixed_eps"],
                                   "iters": ctl["its"][-1], "residual": ctl["res"][-1], "mean_rank": ctl["mean_rank"],
-                                  "max_rank": ctl["max_rank"], "kernel_ms": ctl["kt"][-1]},
+                                  "max_rank": ctl["max_rank"], "kernel_ms": ctl["kt"][-1], "tuning": ctl["tuning"]},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
             "speedup_precision_only": t_ctl / t_mixed,
             "kernel_roofline": {a: kernel_roofline(arms[a], peaks, hbm) for a in ("mixed", "fp64")},
@@ -712,7 +733,9 @@ def main():
                          "frac": achieved / peak64 if peak64 else None,
                          "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in "
                                         "MEASURED_PEAKS.json)",
-                         "traffic": RECOMP_TRAFFIC},
+                         "traffic": RECOMP_BYTES_PER_FLOP * rec["flops"] / (CFG["nb"] - 1),
+                         "traffic_note": "bytes per launch: DRAM bytes per FLOP of the N=8192 capture x the mean "
+                                         "launch's FLOPs"},
             "gpu_launches": mx["stats"]["launches"],
             "clocks": mx["clocks"],
         }

@@ -54,9 +54,12 @@ std::mutex& globals_mutex() {
   return m;
 }
 
+// FRANK_LRA as addition.cpp:191-203 reads it: "naive", "rounded_addition",
+// anything else fast_rounded_addition.  Plans reject "naive" (set_lra fails).
 std::string lra_name() {
   const std::string v = getGlobalValue("FRANK_LRA");
-  return v == "rounded_addition" ? "rounded_addition" : "fast_rounded_addition";
+  if (v == "rounded_addition" || v == "naive") return v;
+  return "fast_rounded_addition";
 }
 
 // Device copy of a Dense (column-major, ld = rows).

@@ -161,8 +161,9 @@ class Hierarchical : public Matrix {
 };
 
 // Global settings (util/global_key_value.h): "FRANK_LRA" selects the LowRank
-// addition ("rounded_addition", else fast_rounded_addition, which falls back
-// to rounded_addition at a tolerance); "FRANK_PRECISION" ("fp64", default, or
+// addition ("naive" -- LowRank += LowRank only, the BLR plans reject it --,
+// "rounded_addition", else fast_rounded_addition, which falls back to
+// rounded_addition at a tolerance); "FRANK_PRECISION" ("fp64", default, or
 // "mixed": FP32 factor, meant for iterative refinement) the plans' arithmetic.
 void setGlobalValue(const std::string key, const std::string value);
 std::string getGlobalValue(const std::string key);

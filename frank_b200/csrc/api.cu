@@ -138,7 +138,7 @@ struct frank_blr {
   // lookahead: second capture stream and its dependency events
   cudaStream_t aux = nullptr;
   cudaEvent_t fork = nullptr;
-  std::vector<cudaEvent_t> getrf_done, dense_done, panel_done;
+  std::vector<cudaEvent_t> getrf_done, dense_done, panel_done, next_done;
 };
 
 namespace {
@@ -230,11 +230,11 @@ int ensure_scratch(frank_blr* p) {
 
 // One factorization on stream s.  After step i's panels, a second stream
 // (p->aux) updates the diagonal block (i+1, i+1), runs the leaf getrf of
-// step i+1 and then updates the step's other dense targets, all overlapping
-// step i's recompressions on s (lookahead of depth one); the main stream
-// waits for the dense updates before the next panels, and for the getrf
-// before the next inverses.  The recompression grid leaves one SM free for
-// the second stream.
+// step i+1 and the explicit inverses of its factors, and then updates the
+// step's other dense targets, all overlapping step i's recompressions on s
+// (lookahead of depth one); the main stream waits for the dense updates and
+// the inverses before the next panels.  The recompression grid leaves one SM
+// free for the second stream.
 template <typename T>
 int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   p->timed = timing;
@@ -245,19 +245,32 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   int64_t launches = 0;
   k_reset<T><<<p->nb * p->nb, 256, 0, s>>>(H, W);
   ++launches;
-  if (pretruncate(p)) {
-    // mixed plans: the factor's tolerance is looser than A_H's, so the working
-    // copy's low-rank blocks are truncated to it before the first step
-    k_truncate_lr<T><<<std::max(p->grid_recomp, p->grid_gram), TRUNC_THREADS, 0, s>>>(
-        H, W, ws, p->core_scale * p->eps, p->rscratch, p->rstride);
-    ++launches;
-  }
   CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
   CUDA_TRY(cudaMemsetAsync(p->work, 0, 2 * p->nb * sizeof(int), s));
   if (p->split_done) CUDA_TRY(cudaMemsetAsync(p->split_done, 0, (size_t)p->nb * SPLIT_MAX * sizeof(int), s));
   CUDA_TRY(cudaEventRecord(p->fork, s));
   CUDA_TRY(cudaStreamWaitEvent(s2, p->fork, 0));
+  if (pretruncate(p)) {
+    // mixed plans: the factor's tolerance is looser than A_H's, so the working
+    // copy's low-rank blocks are truncated to it before the first step (beside
+    // the first leaf getrf, which reads only the dense diagonal block)
+    k_truncate_lr<T><<<std::max(p->grid_recomp, p->grid_gram), TRUNC_THREADS, 0, s>>>(
+        H, W, ws, p->core_scale * p->eps, p->rscratch, p->rstride);
+    ++launches;
+  }
+  // explicit inverses of a step's diagonal factors, all column blocks in
+  // parallel; on the second stream right after the leaf getrf, except in a
+  // replay with timing events (there on the main stream, serialised)
+  auto trinv_on = [&](int step, cudaStream_t st) -> int {
+    const int cw = trinv_width(p->bmax);
+    const int nblk = (int)((p->off_h[step + 1] - p->off_h[step] + cw - 1) / cw);
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_TRINV, 0), st, cudaEventRecordExternal));
+    k_trinv<T><<<2 * nblk, TRINV_THREADS, (size_t)p->bmax * cw * sizeof(double), st>>>(W, ws, step, cw);
+    if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_TRINV, 1), st, cudaEventRecordExternal));
+    ++launches;
+    return FRANK_OK;
+  };
   auto getrf_on_aux = [&](int step) -> int {
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 0), s2, cudaEventRecordExternal));
     {
@@ -278,6 +291,10 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
       launches += 1;
     }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, step, FLOP_GETRF, 1), s2, cudaEventRecordExternal));
+    if (!timing) {
+      const int rc2 = trinv_on(step, s2);
+      if (rc2) return rc2;
+    }
     CUDA_TRY(cudaEventRecord(p->getrf_done[step], s2));
     return FRANK_OK;
   };
@@ -286,15 +303,7 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
   ++launches;   // the getrf load kernel
   for (int i = 0; i < p->nb; ++i) {
     CUDA_TRY(cudaStreamWaitEvent(s, p->getrf_done[i], 0));
-    {
-      // explicit inverses of step i's factors, all column blocks in parallel
-      const int cw = trinv_width(p->bmax);
-      const int nblk = (int)((p->off_h[i + 1] - p->off_h[i] + cw - 1) / cw);
-      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_TRINV, 0), s, cudaEventRecordExternal));
-      k_trinv<T><<<2 * nblk, TRINV_THREADS, (size_t)p->bmax * cw * sizeof(double), s>>>(W, ws, i, cw);
-      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_TRINV, 1), s, cudaEventRecordExternal));
-      ++launches;
-    }
+    if (timing && (rc = trinv_on(i, s))) return rc;
     const int m = p->nb - i - 1;
     if (m == 0) break;
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_PANEL, 0), s, cudaEventRecordExternal));
@@ -313,25 +322,33 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
     // panels): the next diagonal block first, its leaf getrf, then the other
     // dense targets.  The next panel overwrites WL / WU, so the main stream
     // waits for all of it after the recompressions.
+    // A replay with timing events keeps the dense updates on the main stream
+    // (serialised), so that their events time the kernels and not their
+    // overlap with the recompressions.
+    cudaStream_t sd = timing ? s : s2;
     CUDA_TRY(cudaEventRecord(p->panel_done[i], s));
-    CUDA_TRY(cudaStreamWaitEvent(s2, p->panel_done[i], 0));
+    if (sd != s) CUDA_TRY(cudaStreamWaitEvent(sd, p->panel_done[i], 0));
     {
       const int band = std::min(p->dupd_band, p->bmax);
       const int nbands = (p->bmax + band - 1) / band;
-      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 0), s2, cudaEventRecordExternal));
-      k_update_dense<T><<<nbands, DUPD_THREADS, 0, s2>>>(W, ws, i, p->dupd_band, DUPD_NEXT);
-      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 1), s2, cudaEventRecordExternal));
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 0), sd, cudaEventRecordExternal));
+      k_update_dense<T><<<nbands, DUPD_THREADS, 0, sd>>>(W, ws, i, p->dupd_band, DUPD_NEXT);
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 1), sd, cudaEventRecordExternal));
       ++launches;
+      if (sd == s) {
+        CUDA_TRY(cudaEventRecord(p->next_done[i], s));
+        CUDA_TRY(cudaStreamWaitEvent(s2, p->next_done[i], 0));
+      }
       if ((rc = getrf_on_aux(i + 1))) return rc;
       ++launches;   // the getrf load kernel
-      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), s2, cudaEventRecordExternal));
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 0), sd, cudaEventRecordExternal));
       if (m > 1) {
-        k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nbands, p->grid_dense), DUPD_THREADS, 0, s2>>>(
+        k_update_dense<T><<<(int)std::min<int64_t>((int64_t)mm * nbands, p->grid_dense), DUPD_THREADS, 0, sd>>>(
             W, ws, i, p->dupd_band, DUPD_REST);
         ++launches;
       }
-      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), s2, cudaEventRecordExternal));
-      CUDA_TRY(cudaEventRecord(p->dense_done[i], s2));
+      if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_DENSE, 1), sd, cudaEventRecordExternal));
+      CUDA_TRY(cudaEventRecord(p->dense_done[i], sd));
     }
     if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, FLOP_RECOMP, 0), s, cudaEventRecordExternal));
     if (p->nlr > 0) {
@@ -607,6 +624,7 @@ void free_plan(frank_blr* p) {
   for (cudaEvent_t e : p->getrf_done) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : p->dense_done) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : p->panel_done) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->next_done) if (e) cudaEventDestroy(e);
   if (p->fork) cudaEventDestroy(p->fork);
   if (p->aux) cudaStreamDestroy(p->aux);
   if (p->graph_stream) cudaStreamDestroy(p->graph_stream);
@@ -793,7 +811,8 @@ int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_bl
   p->getrf_done.assign(nb, nullptr);
   p->dense_done.assign(nb, nullptr);
   p->panel_done.assign(nb, nullptr);
-  for (auto* v : {&p->getrf_done, &p->dense_done, &p->panel_done})
+  p->next_done.assign(nb, nullptr);
+  for (auto* v : {&p->getrf_done, &p->dense_done, &p->panel_done, &p->next_done})
     for (auto& e : *v)
       if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
         free_plan(p);
@@ -1748,12 +1767,12 @@ extern "C" int frank_debug_tlog(long long* out, unsigned long long* n) {
   return FRANK_OK;
 }
 
-extern "C" int frank_debug_phase_cycles(unsigned long long* cycles16, unsigned long long* count2) {
-  CUDA_TRY(cudaMemcpyFromSymbol(cycles16, g_phase_cycles, sizeof(unsigned long long) * 16));
-  CUDA_TRY(cudaMemcpyFromSymbol(count2, g_phase_count, sizeof(unsigned long long) * 2));
-  unsigned long long z[16] = {0};
+extern "C" int frank_debug_phase_cycles(unsigned long long* cycles24, unsigned long long* count3) {
+  CUDA_TRY(cudaMemcpyFromSymbol(cycles24, g_phase_cycles, sizeof(unsigned long long) * 24));
+  CUDA_TRY(cudaMemcpyFromSymbol(count3, g_phase_count, sizeof(unsigned long long) * 3));
+  unsigned long long z[24] = {0};
   CUDA_TRY(cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z)));
-  CUDA_TRY(cudaMemcpyToSymbol(g_phase_count, z, sizeof(unsigned long long) * 2));
+  CUDA_TRY(cudaMemcpyToSymbol(g_phase_count, z, sizeof(unsigned long long) * 3));
   return FRANK_OK;
 }
 #endif

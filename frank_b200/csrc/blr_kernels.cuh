@@ -35,7 +35,8 @@ struct BlrView {
 };
 
 // Optional per-phase cycle counters of the recompression kernels (build with
-// -DFRANK_PHASE_TIMING; off by default).  Slots: [size class][phase].
+// -DFRANK_PHASE_TIMING; off by default).  Slots: [size class][phase], the
+// classes stacked sizes <= 64, <= 160 and larger.
 #ifdef FRANK_PHASE_TIMING
 __device__ unsigned long long g_getrf_cycles[8];
 #define GPHASE(k)                                                                           \
@@ -52,8 +53,8 @@ __device__ unsigned long long g_getrf_cycles[8];
 #define GPHASE_BEGIN() do {} while (0)
 #endif
 #ifdef FRANK_PHASE_TIMING
-__device__ unsigned long long g_phase_cycles[2][8];
-__device__ unsigned long long g_phase_count[2];
+__device__ unsigned long long g_phase_cycles[3][8];
+__device__ unsigned long long g_phase_count[3];
 #define PHASE_BEGIN() long long _ph_t0 = clock64(); int _ph_last = 0
 #define PHASE_MARK(cls, k)                                                                  \
   do {                                                                                      \
@@ -1122,7 +1123,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       if (threadIdx.x == 0) atomicAdd(ws.err + ERR_BOUNDS, 1);
       continue;
     }
-    const int cls = (su <= 64 && sv <= 64) ? 0 : 1;
+    const int cls = (su <= 64 && sv <= 64) ? 0 : (su <= 160 && sv <= 160 ? 1 : 2);
     PHASE_BEGIN();
 #ifdef FRANK_PHASE_TIMING
     const long long t_start = gtimer();

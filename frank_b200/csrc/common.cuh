@@ -642,10 +642,12 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
     }
     __syncthreads();
     double* col = A + (int64_t)r * lda;
+    // every thread reads alpha before the reduction's barriers, so thread 0
+    // may overwrite col[r] below without a barrier of its own
+    const double alpha = col[r];
     double s = 0.0;
     for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) s += col[e] * col[e];
     const double xn2 = block_sum(s, red);
-    const double alpha = col[r];
     double tt = 0.0, beta = alpha;
     if (xn2 > 0.0) {
       const double nrm = sqrt(alpha * alpha + xn2);
@@ -654,35 +656,60 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
       const double scal = 1.0 / (alpha - beta);
       for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) col[e] *= scal;
     }
-    __syncthreads();
+    // the scaling leaves col[r] alone: one barrier for both
     if (threadIdx.x == 0) { col[r] = beta; tau[r] = tt; }
     __syncthreads();
     if (r < min(m, n) - 1 && tt != 0.0) {
-      for (int c = r + 1 + wid; c < n; c += nw) {
-        double* cc = A + (int64_t)c * lda;
-        double w = (lane == 0) ? cc[r] : 0.0;
-        for (int e = r + 1 + lane; e < m; e += 32) w += col[e] * cc[e];
-        w = warp_sum(w) * tt;
-        if (lane == 0) cc[r] -= w;
-        for (int e = r + 1 + lane; e < m; e += 32) cc[e] -= w * col[e];
+      // four columns per warp pass, so that each lane has four independent
+      // load streams in flight (the trailing matrix is often in L2)
+      for (int c0 = r + 1 + 4 * wid; c0 < n; c0 += 4 * nw) {
+        const int nc = min(4, n - c0);
+        double* p0 = A + (int64_t)c0 * lda;
+        double* p1 = nc > 1 ? p0 + lda : p0;
+        double* p2 = nc > 2 ? p0 + 2 * lda : p0;
+        double* p3 = nc > 3 ? p0 + 3 * lda : p0;
+        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+        if (lane == 0) { w0 = p0[r]; w1 = p1[r]; w2 = p2[r]; w3 = p3[r]; }
+        for (int e = r + 1 + lane; e < m; e += 32) {
+          const double v = col[e];
+          w0 = fma(v, p0[e], w0); w1 = fma(v, p1[e], w1); w2 = fma(v, p2[e], w2); w3 = fma(v, p3[e], w3);
+        }
+        w0 = warp_sum(w0) * tt; w1 = warp_sum(w1) * tt; w2 = warp_sum(w2) * tt; w3 = warp_sum(w3) * tt;
+        if (lane == 0) {
+          p0[r] -= w0;
+          if (nc > 1) p1[r] -= w1;
+          if (nc > 2) p2[r] -= w2;
+          if (nc > 3) p3[r] -= w3;
+        }
+        for (int e = r + 1 + lane; e < m; e += 32) {
+          const double v = col[e];
+          p0[e] -= w0 * v;
+          if (nc > 1) p1[e] -= w1 * v;
+          if (nc > 2) p2[e] -= w2 * v;
+          if (nc > 3) p3[e] -= w3 * v;
+        }
       }
     }
     __syncthreads();
-    for (int c = r + 1 + wid; c < n; c += nw) {
+    // norm down-dating, one column per thread; a column whose down-dated norm
+    // is unreliable is marked (-1) and recomputed by a warp below
+    for (int c = r + 1 + threadIdx.x; c < n; c += blockDim.x) {
       if (cnorm[c] != 0.0) {
         double temp = fabs(A[r + (int64_t)c * lda] / cnorm[c]);
         temp = fmax(0.0, (1.0 - temp) * (1.0 + temp));
         const double ratio = cnorm[c] / partial[c];
         const double temp2 = temp * ratio * ratio;
-        if (temp2 > tol3z) {
-          if (lane == 0) cnorm[c] = cnorm[c] * sqrt(temp);
-        } else {
-          double s2 = 0.0;
-          if (r < m - 1)
-            for (int e = r + 1 + lane; e < m; e += 32) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
-          s2 = warp_sum(s2);
-          if (lane == 0) { cnorm[c] = (r < m - 1) ? sqrt(s2) : 0.0; partial[c] = cnorm[c]; }
-        }
+        cnorm[c] = temp2 > tol3z ? cnorm[c] * sqrt(temp) : -1.0;
+      }
+    }
+    __syncthreads();
+    for (int c = r + 1 + wid; c < n; c += nw) {
+      if (cnorm[c] < 0.0) {
+        double s2 = 0.0;
+        if (r < m - 1)
+          for (int e = r + 1 + lane; e < m; e += 32) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
+        s2 = warp_sum(s2);
+        if (lane == 0) { cnorm[c] = (r < m - 1) ? sqrt(s2) : 0.0; partial[c] = cnorm[c]; }
       }
       __syncwarp();
     }

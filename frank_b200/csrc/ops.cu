@@ -554,6 +554,44 @@ int check_dims(int m, int n, int count, int maxdim = 4096) {
   return FRANK_OK;
 }
 
+// naive_addition (addition.cpp:68-89), concatenation branch: U = [Ua Ub],
+// S = blockdiag(Sa, Sb), V = [Va; Vb] in A's buffers (capacity >= ka + kb).
+__global__ void k_op_lr_concat(int m, int n, int ka, int kb, Mat Ua, Mat Sa, Mat Va, Mat Ub, Mat Sb, Mat Vb,
+                               int b) {
+  double *ua = Ua.at(b), *sa = Sa.at(b), *va = Va.at(b);
+  const double *ub = Ub.at(b), *sb = Sb.at(b), *vb = Vb.at(b);
+  const int kt = ka + kb;
+  for (int64_t e = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; e < (int64_t)m * kb;
+       e += (int64_t)blockDim.x * gridDim.x) {
+    const int r = e % m, c = e / m;
+    ua[r + (int64_t)(ka + c) * Ua.ld] = ub[r + (int64_t)c * Ub.ld];
+  }
+  for (int64_t e = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; e < (int64_t)kb * n;
+       e += (int64_t)blockDim.x * gridDim.x) {
+    const int r = e % kb, c = e / kb;
+    va[ka + r + (int64_t)c * Va.ld] = vb[r + (int64_t)c * Vb.ld];
+  }
+  // S: the new rows / columns (the old ka x ka block stays)
+  for (int64_t e = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; e < (int64_t)kt * kt;
+       e += (int64_t)blockDim.x * gridDim.x) {
+    const int r = e % kt, c = e / kt;
+    if (r < ka && c < ka) continue;
+    sa[r + (int64_t)c * Sa.ld] = (r >= ka && c >= ka) ? sb[(r - ka) + (int64_t)(c - ka) * Sb.ld] : 0.0;
+  }
+}
+
+// naive_addition, recompression branch: D = Ua Sa Va + Ub Sb Vb (m x n, ld m)
+// for LowRank(Dense(A) + Dense(B), ka).
+__global__ void __launch_bounds__(OT) k_op_lr_dense(int m, int n, int ka, int kb, Mat Ua, Mat Sa, Mat Va, Mat Ub,
+                                                    Mat Sb, Mat Vb, int b, double* D, double* T) {
+  __shared__ double gsm[GSM];
+  // T = Ua Sa (m x ka), D = T Va; T = Ub Sb, D += T Vb
+  cta_gemm<double, OT>(m, ka, ka, 1.0, Ua.at(b), Ua.ld, false, Sa.at(b), Sa.ld, false, 0.0, T, m, gsm);
+  cta_gemm<double, OT>(m, n, ka, 1.0, T, m, false, Va.at(b), Va.ld, false, 0.0, D, m, gsm);
+  cta_gemm<double, OT>(m, kb, kb, 1.0, Ub.at(b), Ub.ld, false, Sb.at(b), Sb.ld, false, 0.0, T, m, gsm);
+  cta_gemm<double, OT>(m, n, kb, 1.0, T, m, false, Vb.at(b), Vb.ld, false, 1.0, D, m, gsm);
+}
+
 // Allocate `count` slots of `ws` doubles plus the error words, run, sync, read errors.
 template <typename Launch>
 int run(cudaStream_t s, int count, int64_t ws, Launch launch) {
@@ -743,6 +781,56 @@ int frank_rid_batched(int m, int n, int count, int sample, int k, const double* 
   return rc;
 }
 
+// naive_addition (addition.cpp:68-89) pair by pair: ranks are read to the
+// host; ka + kb >= min(m, n) recompresses Dense(A) + Dense(B) to rank ka by
+// rsvd with sample min(ka + 5, m, n) and the reference's Omega
+// (LowRank(Dense, rank), low_rank.cpp:40-48), else the bases and S are
+// concatenated (rank ka + kb, which must fit kmax).
+static int lowrank_add_naive(int m, int n, int count, int kmax, double* d_ua, int64_t ldua, int64_t sua, double* d_sa,
+                      int64_t ldsa, int64_t ssa, double* d_va, int64_t ldva, int64_t sva, int* d_ka,
+                      const double* d_ub, int64_t ldub, int64_t sub, const double* d_sb, int64_t ldsb, int64_t ssb,
+                      const double* d_vb, int64_t ldvb, int64_t svb, const int* d_kb, cudaStream_t s) {
+  std::vector<int> ka(count), kb(count);
+  OPS_TRY(cudaMemcpyAsync(ka.data(), d_ka, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
+  OPS_TRY(cudaMemcpyAsync(kb.data(), d_kb, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
+  OPS_TRY(cudaStreamSynchronize(s));
+  const Mat Ua{d_ua, ldua, sua}, Sa{d_sa, ldsa, ssa}, Va{d_va, ldva, sva};
+  const Mat Ub{const_cast<double*>(d_ub), ldub, sub}, Sb{const_cast<double*>(d_sb), ldsb, ssb},
+      Vb{const_cast<double*>(d_vb), ldvb, svb};
+  for (int b = 0; b < count; ++b) {
+    if (ka[b] < 1 || kb[b] < 1 || ka[b] > kmax) return set_error(FRANK_ERR_INVALID, "bad lowrank_add ranks");
+    if (ka[b] + kb[b] < std::min(m, n)) {
+      if (ka[b] + kb[b] > kmax)
+        return set_error(FRANK_ERR_RANK_OVERFLOW, "naive_addition: rank ka + kb exceeds the capacity kmax");
+      k_op_lr_concat<<<std::max(1, std::min(64, (int)(((int64_t)(m + n) * (ka[b] + kb[b]) + 255) / 256))), 256, 0,
+                       s>>>(m, n, ka[b], kb[b], Ua, Sa, Va, Ub, Sb, Vb, b);
+      OPS_TRY(cudaGetLastError());
+      ka[b] += kb[b];
+      continue;
+    }
+    const int rank = ka[b], smp = std::min(rank + 5, std::min(m, n));
+    const std::vector<double> om = omega(n, smp);
+    double *d_om = nullptr, *d_dense = nullptr;
+    OPS_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d_om), sizeof(double) * om.size(), s));
+    OPS_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d_dense),
+                            sizeof(double) * ((int64_t)m * n + (int64_t)m * std::max(ka[b], kb[b])), s));
+    OPS_TRY(cudaMemcpyAsync(d_om, om.data(), sizeof(double) * om.size(), cudaMemcpyHostToDevice, s));
+    k_op_lr_dense<<<1, OT, 0, s>>>(m, n, ka[b], kb[b], Ua, Sa, Va, Ub, Sb, Vb, b, d_dense, d_dense + (int64_t)m * n);
+    const int64_t ws = (int64_t)m * smp + (int64_t)std::max(m, n) * smp + (int64_t)n * smp + smp +
+                       (int64_t)smp * smp + smp + (int64_t)smp * n + svd_scratch(smp, n) + 2;
+    int rc = run(s, 1, ws, [&](double* sc, int* err) {
+      k_op_rsvd<<<1, OT, 0, s>>>(m, n, smp, rank, 0, Mat{d_dense, m, 0}, d_om, Mat{d_ua + b * sua, ldua, 0},
+                                 Mat{d_sa + b * ssa, ldsa, 0}, Mat{d_va + b * sva, ldva, 0}, sc, ws, err);
+    });
+    cudaFreeAsync(d_om, s);
+    cudaFreeAsync(d_dense, s);
+    if (rc) return rc;
+  }
+  OPS_TRY(cudaMemcpyAsync(d_ka, ka.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
+  OPS_TRY(cudaStreamSynchronize(s));
+  return FRANK_OK;
+}
+
 int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra, double eps, double* d_ua,
                               int64_t ldua, int64_t sua, double* d_sa, int64_t ldsa, int64_t ssa, double* d_va,
                               int64_t ldva, int64_t sva, int* d_ka, const double* d_ub, int64_t ldub, int64_t sub,
@@ -755,10 +843,13 @@ int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra
     return set_error(FRANK_ERR_INVALID, "bad lowrank_add arguments");
   const std::string name(lra);
   int fast;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (name == "naive" || name == "naive_addition") return lowrank_add_naive(m, n, count, kmax, d_ua, ldua, sua, d_sa, ldsa, ssa, d_va,
+                                                         ldva, sva, d_ka, d_ub, ldub, sub, d_sb, ldsb, ssb, d_vb,
+                                                         ldvb, svb, d_kb, s);
   if (name == "rounded_addition") fast = 0;
   else if (name == "fast_rounded_addition") fast = 1;
   else return set_error(FRANK_ERR_UNSUPPORTED, "lowrank_add: unknown LowRank addition " + name);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int kt = kmax + kb_max, mx = std::max(m, n);
   const int64_t ws = (int64_t)(m + n) * kt + 2 * kt + 5 * (int64_t)kt * kt + kt + (int64_t)mx * kt +
                      svd_scratch(kt, kt) + 2;

@@ -380,8 +380,12 @@ int frank_rid_batched(int m, int n, int count, int sample, int k, const double* 
  * ka x n, capacity kmax), B = Ub Sb Vb (kb <= kb_max); ranks d_ka (in/out) and
  * d_kb per pair.  lra "rounded_addition" (addition.cpp:93-127: QR of both
  * stacked bases, core SVD, rank by find_svd_truncation_rank at eps, or ka when
- * eps = 0) or "fast_rounded_addition" (addition.cpp:133-189: fixed rank, A's
- * bases orthonormal; falls back to rounded_addition when eps > 0).  Replaces
+ * eps = 0), "fast_rounded_addition" (addition.cpp:133-189: fixed rank, A's
+ * bases orthonormal; falls back to rounded_addition when eps > 0) or "naive"
+ * (also "naive_addition"; addition.cpp:68-89: ka + kb >= min(m, n) gives
+ * LowRank(Dense(A) + Dense(B), ka) by rsvd with the reference's Omega, else
+ * the bases and S are concatenated to rank ka + kb, which must fit kmax --
+ * FRANK_ERR_RANK_OVERFLOW otherwise; reads the ranks to the host).  Replaces
  * operator+=(LowRank&, const LowRank&) (addition.cpp:191-203). */
 int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra, double eps, double* d_ua,
                               int64_t ldua, int64_t stride_ua, double* d_sa, int64_t ldsa, int64_t stride_sa,

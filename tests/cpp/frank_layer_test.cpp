@@ -79,6 +79,26 @@ static void lowrank_addition(const char* lra) {
   expect(err < 1e-4 && A.rank == rank, std::string("lowrank += lowrank ") + lra, err);
 }
 
+// FRANK_LRA=naive (addition.cpp:68-89): rank + rank < min(m, n) concatenates
+// (rank 2 * rank, the sum represented exactly)
+static void lowrank_naive() {
+  FRANK::setGlobalValue("FRANK_LRA", "naive");
+  const int64_t m = 64, n = 64, rank = 8;
+  std::vector<std::vector<double>> randx{FRANK::get_sorted_random_vector(2 * n)};
+  const FRANK::Dense D(FRANK::laplacend, randx, m, n, 0, n);
+  FRANK::LowRank A(D, rank);
+  const FRANK::LowRank B(D, rank);
+  A += B;
+  FRANK::Dense sum(m, n), two(m, n), US(m, A.rank);
+  FRANK::gemm(A.U, A.S, US, 1, 0);
+  FRANK::gemm(US, A.V, sum, 1, 0);
+  for (int64_t i = 0; i < m; ++i)
+    for (int64_t j = 0; j < n; ++j) two(i, j) = 2 * D(i, j);
+  const double err = FRANK::l2_error(two, sum);
+  expect(err < 1e-4 && A.rank == 2 * rank, "lowrank += lowrank naive", err);
+  FRANK::setGlobalValue("FRANK_LRA", "");
+}
+
 // test/dense_qr_test.cpp, dense_svd_test.cpp, dense_id_test.cpp (reduced n)
 static void dense_ops() {
   const int64_t n = 256, k = 16;
@@ -143,6 +163,7 @@ int main() {
     for (int64_t rank : {4, 8}) blr_fixed_rank(n, 32, rank, 0.0);
   lowrank_addition("rounded_addition");
   lowrank_addition("fast_rounded_addition");
+  lowrank_naive();
   dense_ops();
   dispatch_errors();
   std::printf("%d failures\n", failures);

@@ -218,6 +218,22 @@ def test_lowrank_add_fixed_rank_matches_oracle(gpu_lib, alg, m, n, rank):
         A = fo.LowRank(U, S, V, r)
 
 
+@pytest.mark.parametrize("m,n,ka,kb", [(64, 64, 4, 4), (64, 21, 8, 16), (48, 48, 20, 30)])
+def test_lowrank_add_naive_matches_oracle(gpu_lib, m, n, ka, kb):
+    """naive_addition (addition.cpp:68-89, FRANK_LRA=naive): concatenation when
+    ka + kb < min(m, n) (exact, rank ka + kb), else LowRank(Dense(A) + Dense(B),
+    ka) by rsvd with the reference's Omega -- equal to the oracle's."""
+    x = np.array([fo.get_sorted_random_vector(3 * max(m, n))])
+    DA = fo.laplacend(x, 0, m, n, n)
+    DB = fo.laplacend(x, 0, m, 2 * n, n)
+    A, B = fo.LowRank.from_rank(DA, ka), fo.LowRank.from_rank(DB, kb)
+    U, S, V, r = _lr_add(gpu_lib, A, B, "naive", 0.0, ka + kb)
+    ref = A.copy()
+    fo.naive_addition(ref, B)
+    assert r == ref.rank == (ka + kb if ka + kb < min(m, n) else ka)
+    np.testing.assert_allclose(U @ S @ V, ref.dense(), rtol=0, atol=1e-10 * np.linalg.norm(DA + DB))
+
+
 @pytest.mark.parametrize("m,n", [(64, 64), (64, 32)])
 @pytest.mark.parametrize("eps", [1e-6, 1e-8, 1e-10])
 def test_lowrank_add_fixed_accuracy_matches_oracle(gpu_lib, m, n, eps):
