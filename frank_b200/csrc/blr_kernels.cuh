@@ -943,13 +943,17 @@ enum CoreMethod { CORE_RRQR = 0, CORE_SVD = 1, CORE_FAST = 2 };
 template <typename T, int NT>
 FRANK_D int svd_core(int mu, int mv, double* Mm, const FactorWs<T>& ws, int kcap, double* region, int64_t cap,
                      double* Atmp, double* tau, double* cnorm, double* partial, int* jpvt, double* sig, int* ord,
-                     double* Xo, int bc, double* Yo, int bk, double* red, int* redi, int* flag, int* s_rank) {
+                     double* Xo, int bc, double* Yo, int bk, double* gsm, double* red, int* redi, int* flag,
+                     int* s_rank) {
   const int nsv = min(mu, mv);
   double f = 0.0;
   for (int64_t e = threadIdx.x; e < (int64_t)mu * mv; e += blockDim.x) f += Mm[e] * Mm[e];
   const double fro = sqrt(block_sum(f, red));
   const double thr = ws.fixed_rank > 0 ? 0.0 : 0.01 * ws.eps * fro / sqrt((double)mv * (double)nsv);
-  const int k = cta_truncated_geqp3(mu, mv, Mm, mu, thr, nsv, tau, cnorm, partial, jpvt, red, redi);
+  // a core in L2 takes the blocked pivoted QR (F, mv x 32, in Atmp)
+  const int k = Mm != region ? cta_truncated_geqp3_blocked<NT>(mu, mv, Mm, mu, thr, nsv, tau, cnorm, partial, jpvt,
+                                                               red, redi, Atmp, gsm)
+                             : cta_truncated_geqp3(mu, mv, Mm, mu, thr, nsv, tau, cnorm, partial, jpvt, red, redi);
   // [A; I] with A = R(0:k, :)^T (mv x k), ld mv + k
   const int ldj = mv + k;
   const int64_t off = (Mm == region) ? (int64_t)mu * mv : 0;
@@ -1148,6 +1152,9 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       else v = double(o.YR[(c - kc) + (int64_t)r * ld]);  // A(i,k)^T
       Bsh[r + (int64_t)c * bk] = v;
     }
+    // the stacked bases are read across threads below (the V side of a split
+    // target forms no core, whose barrier would otherwise cover this)
+    __syncthreads();
     SUB_MARK(9);
     if (do_u) form_core<T, RECOMP_THREADS>(o, bi, ld, Tm, gsm);
     SUB_MARK(10);
@@ -1234,7 +1241,13 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       double* cn = in_smem ? region + (int64_t)mu * mv : cnorm;
       double* pn = in_smem ? cn + mv : pnorm;
       double* tc = in_smem ? pn + mv : tau_c;
-      r = cta_truncated_geqp3(mu, mv, Mm, mu, core_scale * ws.eps * sqrt(f), A.kcap, tc, cn, pn, jpvt, red, redi);
+      // a core in L2 (too large for shared memory) takes the blocked pivoted
+      // QR, its F matrix (mv x 32) in Mtmp (free until the RQ below)
+      const double thr_c = core_scale * ws.eps * sqrt(f);
+      r = (!in_smem && (int64_t)mv * 32 <= L.mglob - L.mtmp)
+              ? cta_truncated_geqp3_blocked<RECOMP_THREADS>(mu, mv, Mm, mu, thr_c, A.kcap, tc, cn, pn, jpvt, red, redi,
+                                                            Mtmp, gsm)
+              : cta_truncated_geqp3(mu, mv, Mm, mu, thr_c, A.kcap, tc, cn, pn, jpvt, red, redi);
       if (r == 0) {
         // zero core: rank-1 zero block (geqp3.cpp:97-102)
         if (threadIdx.x == 0) { atomicMax(ws.err + ERR_MAX_RANK, 1); atomicAdd(ws.err + ERR_RECOMP, 1); }
@@ -1304,7 +1317,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     } else {
       // SVD core (Rc / Rv are free once the core is formed: Jacobi scratch)
       r = svd_core<T, RECOMP_THREADS>(mu, mv, Mm, ws, A.kcap, region, RECOMP_REGION, Rc, tau_c, cnorm, pnorm, jpvt,
-                                      tau2, jinv, Xo, bc, Yo, bk, red, redi, &flag, &s_rank);
+                                      tau2, jinv, Xo, bc, Yo, bk, gsm, red, redi, &flag, &s_rank);
       for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
         const int rr = e % r, c = e / r;
         Sc[rr + (int64_t)c * A.kcap] = T(rr == c ? pnorm[c] : 0.0);

@@ -724,6 +724,191 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
   return r;
 }
 
+
+// ---------------------------------------------------------------------------
+// The same truncated column-pivoted QR (same pivots, same stopping rule and
+// norm down-dating) blocked as LAPACK's dlaqps: QB pivot steps per panel, each
+// step updating only its pivot column and pivot row from the panel's
+// reflectors and an n x QB matrix F (F(:, k) = tau_k A^T v_k, corrected for
+// the panel's earlier reflectors), the trailing matrix updated once per panel
+// as A -= V F^T (a CTA GEMM).  A step reads the trailing matrix once instead
+// of reading and writing it, which is what bounds a core too large for shared
+// memory (it lives in L2).  A column whose down-dated norm is unreliable ends
+// the panel; its norm is recomputed after the trailing update.  F: n x QB
+// doubles (ld n), anywhere; red holds the panel's auxiliary vector between
+// the reflector and the next pivot search.  Returns the rank r.
+// ---------------------------------------------------------------------------
+template <int NT>
+FRANK_D int cta_truncated_geqp3_blocked(int m, int n, double* A, int64_t lda, double thr, int maxr, double* tau,
+                                        double* cnorm, double* partial, int* jpvt, double* red, int* redi,
+                                        double* F, double* gsm) {
+  constexpr int QB = 32;
+  const double dlamch_e = 1.1102230246251565e-16;
+  const double tol3z = sqrt(dlamch_e);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int mind = min(min(m, n), maxr);
+  for (int c = wid; c < n; c += nw) {
+    double s = 0.0;
+    for (int r = lane; r < m; r += 32) s += A[r + (int64_t)c * lda] * A[r + (int64_t)c * lda];
+    s = warp_sum(s);
+    if (lane == 0) { cnorm[c] = sqrt(s); partial[c] = sqrt(s); jpvt[c] = c; }
+  }
+  __syncthreads();
+  double maxc;
+  int kp_next;
+  {
+    double best = -1.0; int bi = -1;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+    kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+  }
+  int r = 0;
+  while (r < mind && maxc > thr) {
+    const int j0 = r;
+    const int kbmax = min(QB, mind - j0);
+    int k = 0;
+    bool recompute = false;
+    while (k < kbmax && maxc > thr) {
+      const int j = j0 + k;
+      const int kp = kp_next;
+      if (kp != j) {
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {
+          const double a = A[e + (int64_t)j * lda];
+          A[e + (int64_t)j * lda] = A[e + (int64_t)kp * lda];
+          A[e + (int64_t)kp * lda] = a;
+        }
+        for (int t = threadIdx.x; t < k; t += blockDim.x) {
+          const double a = F[j + (int64_t)t * n];
+          F[j + (int64_t)t * n] = F[kp + (int64_t)t * n];
+          F[kp + (int64_t)t * n] = a;
+        }
+        if (threadIdx.x == 0) {
+          double a = cnorm[j]; cnorm[j] = cnorm[kp]; cnorm[kp] = a;
+          a = partial[j]; partial[j] = partial[kp]; partial[kp] = a;
+          int q = jpvt[j]; jpvt[j] = jpvt[kp]; jpvt[kp] = q;
+        }
+      }
+      __syncthreads();
+      double* col = A + (int64_t)j * lda;
+      // pivot column, rows j.. : the panel's earlier reflectors (rows above j
+      // were brought up to date by the earlier pivot-row updates)
+      if (k > 0) {
+        for (int e = j + threadIdx.x; e < m; e += blockDim.x) {
+          double s = 0.0;
+          for (int t = 0; t < k; ++t) s += A[e + (int64_t)(j0 + t) * lda] * F[j + (int64_t)t * n];
+          col[e] -= s;
+        }
+        __syncthreads();
+      }
+      const double alpha = col[j];
+      double s = 0.0;
+      for (int e = j + 1 + threadIdx.x; e < m; e += blockDim.x) s += col[e] * col[e];
+      const double xn2 = block_sum(s, red);
+      double tt = 0.0, beta = alpha;
+      if (xn2 > 0.0) {
+        const double nrm = sqrt(alpha * alpha + xn2);
+        beta = alpha >= 0.0 ? -nrm : nrm;
+        tt = (beta - alpha) / beta;
+        const double scal = 1.0 / (alpha - beta);
+        for (int e = j + 1 + threadIdx.x; e < m; e += blockDim.x) col[e] *= scal;
+      }
+      // the reflector's unit entry in place while F and the pivot row are formed
+      if (threadIdx.x == 0) { col[j] = 1.0; tau[j] = tt; }
+      __syncthreads();
+      // F(c, k) = tt A(j:m, c)^T v for c > j (four columns per warp pass), 0 above
+      for (int c0 = j + 1 + 4 * wid; c0 < n; c0 += 4 * nw) {
+        const int nc = min(4, n - c0);
+        const double* p0 = A + (int64_t)c0 * lda;
+        const double* p1 = nc > 1 ? p0 + lda : p0;
+        const double* p2 = nc > 2 ? p0 + 2 * lda : p0;
+        const double* p3 = nc > 3 ? p0 + 3 * lda : p0;
+        double w0 = 0.0, w1 = 0.0, w2 = 0.0, w3 = 0.0;
+        for (int e = j + lane; e < m; e += 32) {
+          const double v = col[e];
+          w0 = fma(v, p0[e], w0); w1 = fma(v, p1[e], w1); w2 = fma(v, p2[e], w2); w3 = fma(v, p3[e], w3);
+        }
+        w0 = warp_sum(w0); w1 = warp_sum(w1); w2 = warp_sum(w2); w3 = warp_sum(w3);
+        if (lane == 0) {
+          double* fk = F + (int64_t)k * n + c0;
+          fk[0] = tt * w0;
+          if (nc > 1) fk[1] = tt * w1;
+          if (nc > 2) fk[2] = tt * w2;
+          if (nc > 3) fk[3] = tt * w3;
+        }
+      }
+      for (int c = threadIdx.x; c <= j && c < n; c += blockDim.x) F[c + (int64_t)k * n] = 0.0;
+      // aux(t) = -tt A(j:m, j0+t)^T v for the panel's earlier reflectors
+      for (int t = wid; t < k; t += nw) {
+        const double* pt = A + (int64_t)(j0 + t) * lda;
+        double w = 0.0;
+        for (int e = j + lane; e < m; e += 32) w = fma(pt[e], col[e], w);
+        w = warp_sum(w);
+        if (lane == 0) red[t] = -tt * w;
+      }
+      __syncthreads();
+      if (k > 0) {
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+          double a = 0.0;
+          for (int t = 0; t < k; ++t) a += F[c + (int64_t)t * n] * red[t];
+          F[c + (int64_t)k * n] += a;
+        }
+        __syncthreads();
+      }
+      // pivot row j: A(j, c) -= A(j, j0:j+1) F(c, 0:k+1)^T for c > j
+      for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) {
+        double a = 0.0;
+        for (int t = 0; t <= k; ++t) a += A[j + (int64_t)(j0 + t) * lda] * F[c + (int64_t)t * n];
+        A[j + (int64_t)c * lda] -= a;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) col[j] = beta;
+      // norm down-dating from the updated pivot row; unreliable ones marked
+      for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) {
+        if (cnorm[c] != 0.0) {
+          double temp = fabs(A[j + (int64_t)c * lda] / cnorm[c]);
+          temp = fmax(0.0, (1.0 - temp) * (1.0 + temp));
+          const double ratio = cnorm[c] / partial[c];
+          const double temp2 = temp * ratio * ratio;
+          cnorm[c] = temp2 > tol3z ? cnorm[c] * sqrt(temp) : -1.0;
+        }
+      }
+      __syncthreads();
+      ++k;
+      // next pivot; a marked column ends the panel (reported as an infinite norm)
+      double best = -1.0; int bi = -1;
+      for (int c = j + 1 + threadIdx.x; c < n; c += blockDim.x) {
+        const double v = cnorm[c] < 0.0 ? INFINITY : cnorm[c];
+        if (v > best) { best = v; bi = c; }
+      }
+      kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+      if (j + 1 >= n) maxc = 0.0;
+      if (isinf(maxc)) { recompute = true; break; }
+    }
+    r = j0 + k;
+    // trailing matrix: A(r:m, r:n) -= A(r:m, j0:r) F(r:n, 0:k)^T
+    if (k > 0 && r < m && r < n)
+      cta_gemm<double, NT>(m - r, n - r, k, -1.0, A + r + (int64_t)j0 * lda, lda, false, F + r, n, true, 1.0,
+                           A + r + (int64_t)r * lda, lda, gsm);
+    if (recompute) {
+      for (int c = r + wid; c < n; c += nw) {
+        if (cnorm[c] < 0.0) {
+          double s2 = 0.0;
+          for (int e = r + lane; e < m; e += 32) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
+          s2 = warp_sum(s2);
+          if (lane == 0) { cnorm[c] = r < m ? sqrt(s2) : 0.0; partial[c] = cnorm[c]; }
+        }
+      }
+      __syncthreads();
+      double best = -1.0; int bi = -1;
+      for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
+      kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+      if (r >= n) maxc = 0.0;
+    }
+    if (k == 0) break;
+  }
+  __syncthreads();
+  return r;
+}
+
 }  // namespace frank
 
 namespace frank {
