@@ -1074,10 +1074,15 @@ int frank_blr_get_pivots(const frank_blr* p, int i, int* ipiv) {
 int frank_blr_set_lra(frank_blr* p, const char* name, double core_scale) {
   if (!p || !name) return fail(FRANK_ERR_INVALID, "null argument");
   const std::string n(name);
-  // addition.cpp:191-203: "rounded_addition" selects it for every plan; any
-  // other value selects fast_rounded_addition, which falls back to
-  // rounded_addition on tolerance plans (addition.cpp:138-143)
+  // addition.cpp:191-203: "rounded_addition" selects it for every plan;
+  // "fast_rounded_addition" (the reference's default) falls back to
+  // rounded_addition on tolerance plans (addition.cpp:138-143); the engine's
+  // RRQR cores are selected by name; "naive" is refused (its ranks grow
+  // without bound, a plan's rank capacity is fixed)
   bool proj = false;
+  if (n == "naive" || n == "naive_addition")
+    return fail(FRANK_ERR_UNSUPPORTED, "naive addition needs unbounded ranks; a plan has a fixed rank capacity "
+                                       "(frank_lowrank_add_batched supports it)");
   if (n == "rounded_addition") { p->core_method = CORE_SVD; p->core_fixed = CORE_SVD; p->gram = false; }
   else if (n == "fast_rounded_addition") { p->core_method = CORE_SVD; p->core_fixed = CORE_FAST; p->gram = false; }
   else if (n == "rounded_addition_rrqr") { p->core_method = CORE_RRQR; p->core_fixed = CORE_SVD; p->gram = false; }

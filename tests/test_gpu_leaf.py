@@ -109,3 +109,9 @@ def test_state_and_argument_errors(gpu_lib):
     with pytest.raises(FrankError) as e:
         M.set_dense(0, 1, np.eye(8))
     assert e.value.code == FRANK_ERR_INVALID
+    # naive addition (FRANK_LRA=naive) grows ranks without bound: plans refuse it
+    from frank_b200._abi import FRANK_ERR_UNSUPPORTED
+    for name in ("naive", "no_such_addition"):
+        with pytest.raises(FrankError) as e:
+            M.set_lra(name)
+        assert e.value.code == FRANK_ERR_UNSUPPORTED
