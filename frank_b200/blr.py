@@ -165,8 +165,10 @@ class BLRMatrix:
     def set_lra(self, name: str, core_scale: float = 0.1):
         """FRANK_LRA: "rounded_addition" (core SVD, the reference algorithm),
         "fast_rounded_addition" (default of fixed-rank plans; tolerance plans
-        fall back to rounded_addition) or "rounded_addition_rrqr"
-        (truncated_geqp3 + rq of the core, default of tolerance plans)."""
+        fall back to rounded_addition), "rounded_addition_rrqr"
+        (truncated_geqp3 + rq of the core on stacked bases) or
+        "rounded_addition_rrqr_proj" (the same on projected bases, default of
+        tolerance plans)."""
         check(lib().frank_blr_set_lra(self._h, name.encode(), float(core_scale)), "frank_blr_set_lra")
 
     def getrf(self, stream: Optional[int] = None, allow=()):

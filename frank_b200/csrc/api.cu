@@ -88,7 +88,8 @@ struct frank_blr {
   int grid_dense = 0, grid_recomp = 0, smax = 0;
   int core_method = CORE_RRQR;   // core of tolerance plans
   int core_fixed = CORE_FAST;    // core of fixed-rank plans (FRANK_LRA unset: fast_rounded_addition)
-  bool proj_tol = false;         // tolerance plans: projected bases (QR of the update's remainder only)
+  bool proj_tol = true;          // tolerance plans: projected bases (QR of the update's remainder only)
+  bool orth_pending = false;     // caller-given low-rank blocks not yet given orthonormal bases
   // launch parameters the autotuner chooses (frank_blr_autotune)
   int dupd_band = DUPD_BAND;     // rows per dense-update task
   int split_p = SPLIT_P;         // split band-1 targets above this operand rank (0: never)
@@ -225,6 +226,21 @@ int ensure_scratch(frank_blr* p) {
   if (p->nlr > 0 && !p->rscratch)
     CUDA_TRY(dalloc(&p->rscratch, (size_t)std::max(p->grid_recomp, p->precision == FRANK_PREC_MIXED ? p->grid_gram : 0) *
                                       p->rstride));
+  return FRANK_OK;
+}
+
+// Orthonormal bases for the caller's low-rank blocks of A_H (once after
+// frank_blr_set_lowrank calls, before the next factorization).
+int orthonormalize_inputs(frank_blr* p, cudaStream_t s) {
+  if (!p->orth_pending || p->nlr == 0) { p->orth_pending = false; return FRANK_OK; }
+  int rc = ensure_scratch(p);
+  if (rc) return rc;
+  const int64_t need = 2 * ((int64_t)p->bmax + p->kcap) * p->kcap + 3 * (int64_t)p->kcap * p->kcap + 2 * p->kcap;
+  if (need > p->rstride) return fail(FRANK_ERR_INVALID, "orthonormalisation scratch");
+  k_orthonormalize_lr<<<p->grid_recomp, ORTH_THREADS, 0, s>>>(h_view(p), p->rscratch, p->rstride);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(s));
+  p->orth_pending = false;
   return FRANK_OK;
 }
 
@@ -417,6 +433,10 @@ int finish_factor(frank_blr* p) {
 
 template <typename T>
 int run_factor(frank_blr* p, cudaStream_t s) {
+  {
+    int rc0 = orthonormalize_inputs(p, s);
+    if (rc0) return rc0;
+  }
   if (!p->graph_exec) {
     // Capture the whole step sequence once; kernel arguments are fixed
     // device pointers, ranks are read from device tables at run time.
@@ -911,6 +931,7 @@ int frank_blr_set_lowrank(frank_blr* p, int i, int j, int rank, const double* U,
   CUDA_TRY(cudaMemcpy(p->Hv + s * bm * kc, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(p->d_rankH + i * p->nb + j, &rank, sizeof(int), cudaMemcpyHostToDevice));
   p->factored = false;
+  p->orth_pending = true;
   return FRANK_OK;
 }
 
@@ -1672,6 +1693,10 @@ int batch_capture(frank_batch* B) {
 extern "C" int frank_batch_getrf(frank_batch* B, void* stream) {
   if (!B) return fail(FRANK_ERR_INVALID, "null batch");
   (void)stream;
+  for (frank_blr* p : B->plans) {
+    int rc = orthonormalize_inputs(p, B->stream);
+    if (rc) return rc;
+  }
   if (!B->exec) {
     int rc = B->plans[0]->precision == FRANK_PREC_FP64 ? batch_capture<double>(B) : batch_capture<float>(B);
     if (rc) return rc;

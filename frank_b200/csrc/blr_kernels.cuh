@@ -175,6 +175,64 @@ __global__ void k_reset(BlrView<double> H, BlrView<T> W) {
 // ---------------------------------------------------------------------------
 constexpr int TRUNC_THREADS = 256;
 
+// Orthonormal bases for low-rank blocks given by the caller
+// (frank_blr_set_lowrank): U = Qu Ru and V^T = Qv Rv by Householder QR, stored
+// as U <- Qu, V^T <- Qv, S <- Ru S Rv^T -- the same matrix, with the
+// orthonormal bases that the reset truncation and the projected additions
+// assume (the on-device constructions produce them already).  One CTA per
+// block at a time; scratch per CTA: 2 (bmax + kcap) kcap + 3 kcap^2 doubles.
+constexpr int ORTH_THREADS = 256;
+__global__ void __launch_bounds__(ORTH_THREADS) k_orthonormalize_lr(BlrView<double> H, double* scratch,
+                                                                   int64_t stride) {
+  __shared__ double gsm[2 * 16 * 64];
+  __shared__ double red[32];
+  double* base = scratch + (int64_t)blockIdx.x * stride;
+  const int nblk = H.nb * H.nb;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    if (H.lslot[blk] < 0) continue;
+    const int k = H.rank[blk];
+    const int i = blk / H.nb, j = blk % H.nb;
+    const int bi = H.bs(i), bj = H.bs(j);
+    if (k < 1 || k > bi || k > bj) continue;
+    double* A1 = base;                        // bi x k, then its reflectors
+    double* A2 = A1 + (int64_t)bi * k;        // bj x k
+    double* Q = A2 + (int64_t)bj * k;         // max(bi, bj) x k
+    double* Ru = Q + (int64_t)max(bi, bj) * k;
+    double* Rv = Ru + (int64_t)k * k;
+    double* Tmp = Rv + (int64_t)k * k;
+    double* tu = Tmp + (int64_t)k * k;
+    double* tv = tu + k;
+    double* hu = H.u(i, j);
+    double* hv = H.vt(i, j);
+    double* hs = H.s(i, j);
+    for (int64_t e = threadIdx.x; e < (int64_t)bi * k; e += blockDim.x) A1[e] = hu[(e % bi) + (e / bi) * H.bmax];
+    for (int64_t e = threadIdx.x; e < (int64_t)bj * k; e += blockDim.x) A2[e] = hv[(e % bj) + (e / bj) * H.bmax];
+    __syncthreads();
+    cta_householder_qr(bi, k, A1, bi, tu, red);
+    cta_householder_qr(bj, k, A2, bj, tv, red);
+    for (int64_t e = threadIdx.x; e < (int64_t)k * k; e += blockDim.x) {
+      const int r = e % k, c = e / k;
+      Ru[e] = r <= c ? A1[r + (int64_t)c * bi] : 0.0;
+      Rv[e] = r <= c ? A2[r + (int64_t)c * bj] : 0.0;
+    }
+    __syncthreads();
+    // S <- Ru S Rv^T
+    cta_gemm<double, ORTH_THREADS>(k, k, k, 1.0, Ru, k, false, hs, H.kcap, false, 0.0, Tmp, k, gsm);
+    cta_gemm<double, ORTH_THREADS>(k, k, k, 1.0, Tmp, k, false, Rv, k, true, 0.0, hs, H.kcap, gsm);
+    // U <- Qu, V^T <- Qv (explicit, from the reflectors)
+    for (int side = 0; side < 2; ++side) {
+      const int m = side ? bj : bi;
+      const double* R = side ? A2 : A1;
+      for (int64_t e = threadIdx.x; e < (int64_t)m * k; e += blockDim.x) Q[e] = ((e % m) == (e / m)) ? 1.0 : 0.0;
+      __syncthreads();
+      cta_apply_q(m, k, R, m, side ? tv : tu, k, Q, (int64_t)m);
+      double* out = side ? hv : hu;
+      for (int64_t e = threadIdx.x; e < (int64_t)m * k; e += blockDim.x) out[(e % m) + (e / m) * H.bmax] = Q[e];
+      __syncthreads();
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr(BlrView<double> H, BlrView<T> W, FactorWs<T> ws,
                                                               double thr_scale, double* scratch, int64_t stride) {

@@ -92,6 +92,46 @@ FRANK_D int block_argmax_abs(double v, int idx, double* redv, int* redi, double*
   return r;
 }
 
+// One-barrier variants of block_sum / block_argmax_abs for the pivoted QR's
+// per-step reductions: each warp's partial goes to red, and after the barrier
+// every thread combines the nw partials itself (same order everywhere, so all
+// threads agree).  The caller must pass another block barrier before red is
+// written again (the pivoted QR's steps do).
+FRANK_D double block_sum1(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < nw; ++w) t += red[w];
+  return t;
+}
+
+FRANK_D int block_argmax_abs1(double v, int idx, double* redv, int* redi, double* absval) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  double a = fabs(v);
+  if (idx < 0) a = -1.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double oa = __shfl_xor_sync(0xffffffffu, a, o);
+    int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (oa > a || (oa == a && oi >= 0 && (idx < 0 || oi < idx))) { a = oa; idx = oi; }
+  }
+  if (lane == 0) { redv[wid] = a; redi[wid] = idx; }
+  __syncthreads();
+  a = -1.0;
+  idx = -1;
+  for (int w = 0; w < nw; ++w) {
+    const double oa = redv[w];
+    const int oi = redi[w];
+    if (oa > a || (oa == a && oi >= 0 && (idx < 0 || oi < idx))) { a = oa; idx = oi; }
+  }
+  *absval = a;
+  return idx;
+}
+
 // ---------------------------------------------------------------------------
 // CTA-wide GEMM: C(m x n) = alpha * op(A) * op(B) + beta * C, column-major.
 // op(A) is m x k: A is (m x k, lda) when !ta, (k x m, lda) when ta.
@@ -647,7 +687,7 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
     const double alpha = col[r];
     double s = 0.0;
     for (int e = r + 1 + threadIdx.x; e < m; e += blockDim.x) s += col[e] * col[e];
-    const double xn2 = block_sum(s, red);
+    const double xn2 = block_sum1(s, red);
     double tt = 0.0, beta = alpha;
     if (xn2 > 0.0) {
       const double nrm = sqrt(alpha * alpha + xn2);
@@ -717,7 +757,7 @@ FRANK_D int cta_truncated_geqp3(int m, int n, double* A, int64_t lda, double thr
     ++r;
     best = -1.0; bi = -1;
     for (int c = r + threadIdx.x; c < n; c += blockDim.x) if (cnorm[c] > best) { best = cnorm[c]; bi = c; }
-    kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+    kp_next = block_argmax_abs1(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
     if (r >= n) maxc = 0.0;
   }
   __syncthreads();
@@ -802,7 +842,7 @@ FRANK_D int cta_truncated_geqp3_blocked(int m, int n, double* A, int64_t lda, do
       const double alpha = col[j];
       double s = 0.0;
       for (int e = j + 1 + threadIdx.x; e < m; e += blockDim.x) s += col[e] * col[e];
-      const double xn2 = block_sum(s, red);
+      const double xn2 = block_sum1(s, red);
       double tt = 0.0, beta = alpha;
       if (xn2 > 0.0) {
         const double nrm = sqrt(alpha * alpha + xn2);
@@ -879,7 +919,7 @@ FRANK_D int cta_truncated_geqp3_blocked(int m, int n, double* A, int64_t lda, do
         const double v = cnorm[c] < 0.0 ? INFINITY : cnorm[c];
         if (v > best) { best = v; bi = c; }
       }
-      kp_next = block_argmax_abs(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
+      kp_next = block_argmax_abs1(best < 0 ? 0.0 : best, bi, red, redi, &maxc);
       if (j + 1 >= n) maxc = 0.0;
       if (isinf(maxc)) { recompute = true; break; }
     }

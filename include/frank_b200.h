@@ -151,14 +151,18 @@ int frank_blr_get_pivots(const frank_blr* plan, int i, int* ipiv);
  *                            orthonormal ones, QR of the remainders only, core
  *                            SVD; on tolerance plans it falls back to
  *                            "rounded_addition" like the reference;
- *   "rounded_addition_rrqr"  (default of tolerance plans) the reference's fixed-accuracy compressor
+ *   "rounded_addition_rrqr"  the reference's fixed-accuracy compressor
  *                            truncated_geqp3 + rq applied to the same core, with
  *                            tolerance core_scale * eps (core_scale <= 0: 0.1);
- *   "rounded_addition_rrqr_proj"  the same RRQR core on projected bases: the
- *                            target's orthonormal U_C, V_C are kept and only the
- *                            update's bases, projected out of them (twice),
- *                            are QR-factored (fast_rounded_addition's bases,
- *                            addition.cpp:133-189, at a tolerance);
+ *   "rounded_addition_rrqr_proj"  (default of tolerance plans) the same RRQR
+ *                            core on projected bases: the target's orthonormal
+ *                            U_C, V_C are kept and only the update's bases,
+ *                            projected out of them (twice), are QR-factored
+ *                            (fast_rounded_addition's bases, addition.cpp:
+ *                            133-189, at a tolerance).  Low-rank blocks given
+ *                            by frank_blr_set_lowrank get orthonormal bases
+ *                            (U = Qu Ru, V^T = Qv Rv, S <- Ru S Rv^T: the same
+ *                            matrix) before the next factorization;
  *   "rounded_addition_rrqr_gram"  mixed plans only: the same RRQR core, with the
  *                            stacked bases orthogonalised through their FP64
  *                            Gram matrices (pivoted Cholesky) instead of a
