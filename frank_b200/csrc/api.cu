@@ -748,6 +748,13 @@ int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_bl
     if (p->off_h[i + 1] - p->off_h[i] <= 0) { delete p; return fail(FRANK_ERR_INVALID, "empty block from the split"); }
   p->bmax = (int)child;
   if (p->bmax > 1024) { delete p; return fail(FRANK_ERR_UNSUPPORTED, "block size above 1024"); }
+  // the recompression's Householder panels (bmax x 32 doubles plus their T
+  // factor) live in shared memory
+  if ((int64_t)p->bmax * QRB + QRB * QRB > RECOMP_REGION) {
+    delete p;
+    return fail(FRANK_ERR_UNSUPPORTED, "block size above " + std::to_string((RECOMP_REGION - QRB * QRB) / QRB) +
+                                           " (recompression panels in shared memory)");
+  }
   p->kcap = d->max_rank > 0 ? std::min(d->max_rank, p->bmax) : p->bmax;
   if (p->fixed_rank > p->kcap) p->kcap = std::min(p->fixed_rank, p->bmax);
   const int nb = d->nb;

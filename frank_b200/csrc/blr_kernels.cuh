@@ -1299,12 +1299,13 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
       double* cn = in_smem ? region + (int64_t)mu * mv : cnorm;
       double* pn = in_smem ? cn + mv : pnorm;
       double* tc = in_smem ? pn + mv : tau_c;
-      // a core in L2 (too large for shared memory) takes the blocked pivoted
-      // QR, its F matrix (mv x 32) in Mtmp (free until the RQ below)
+      // a core in L2 (too large for shared memory) takes the pivoted QR with
+      // randomized block pivoting (panel GEMMs instead of one pass over the
+      // core per column), its scratch in Mtmp (free until the RQ below)
       const double thr_c = core_scale * ws.eps * sqrt(f);
-      r = (!in_smem && (int64_t)mv * 32 <= L.mglob - L.mtmp)
-              ? cta_truncated_geqp3_blocked<RECOMP_THREADS>(mu, mv, Mm, mu, thr_c, A.kcap, tc, cn, pn, jpvt, red, redi,
-                                                            Mtmp, gsm)
+      r = (!in_smem && rqrcp_scratch(mu, mv) <= L.mglob - L.mtmp)
+              ? cta_rand_qrcp<RECOMP_THREADS>(mu, mv, Mm, mu, thr_c, A.kcap, tc, jpvt, Mtmp, smP, smT, gsm, red,
+                                              redi)
               : cta_truncated_geqp3(mu, mv, Mm, mu, thr_c, A.kcap, tc, cn, pn, jpvt, red, redi);
       if (r == 0) {
         // zero core: rank-1 zero block (geqp3.cpp:97-102)
@@ -1340,7 +1341,15 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
           Xo[e] = (rr == c) ? 1.0 : 0.0;
         }
         __syncthreads();
-        cta_apply_q(mu, r, Mm, mu, tc, r, Xo, (int64_t)bc);
+        if (!in_smem) {
+          // a core in L2: the reflectors in panels of QRB (T factors in M0,
+          // free in this branch), applied as blocked WY -- one reflector at a
+          // time would sweep the r x r block once per reflector
+          cta_form_t(mu, r, Mm, mu, tc, M0, smP, smT);
+          cta_apply_q_blocked<RECOMP_THREADS>(mu, r, Mm, mu, M0, r, Xo, (int64_t)bc, Wq, smP, smT, gsm, r);
+        } else {
+          cta_apply_q(mu, r, Mm, mu, tc, r, Xo, (int64_t)bc);
+        }
       }
       // X2 (mv x r) = R_perm^T J, R_perm[:, jpvt[c']] = R[:, c']
       for (int c = threadIdx.x; c < mv; c += blockDim.x) jinv[jpvt[c]] = c;
@@ -1352,7 +1361,8 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
         X2[e] = (row <= src) ? Mm[row + (int64_t)src * mu] : 0.0;
       }
       __syncthreads();
-      cta_householder_qr(mv, r, X2, mv, tau2, red);
+      if (!in_smem) cta_qr_blocked<RECOMP_THREADS>(mv, r, X2, mv, tau2, M0, Wq, smP, smT, gsm, red);
+      else cta_householder_qr(mv, r, X2, mv, tau2, red);
       // S = J Rt^T J (upper triangular)
       for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
         const int a = e % r, c = e / r;
@@ -1366,7 +1376,10 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
         Qt[e] = (rr == c) ? 1.0 : 0.0;
       }
       __syncthreads();
-      cta_apply_q(mv, r, X2, mv, tau2, r, Qt, (int64_t)mv);
+      if (!in_smem)
+        cta_apply_q_blocked<RECOMP_THREADS>(mv, r, X2, mv, M0, r, Qt, (int64_t)mv, Wq, smP, smT, gsm, r);
+      else
+        cta_apply_q(mv, r, X2, mv, tau2, r, Qt, (int64_t)mv);
       for (int64_t e = threadIdx.x; e < (int64_t)bk * r; e += blockDim.x) {
         const int rr = e % bk, a = e / bk;
         Yo[e] = (rr < mv) ? Qt[rr + (int64_t)(r - 1 - a) * mv] : 0.0;

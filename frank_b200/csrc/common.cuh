@@ -530,11 +530,12 @@ __device__ unsigned long long g_sub_cycles[16];
 
 template <int NT>
 FRANK_D void cta_qr_blocked(int m, int n, double* A, int64_t lda, double* tau, double* Tf, double* W,
-                            double* smP, double* smT, double* gsm, double* red) {
+                            double* smP, double* smT, double* gsm, double* red, int max_panels = 1 << 20,
+                            int max_jn = QRB) {
   const int kmin = m < n ? m : n;
   SUB_BEGIN();
-  for (int j0 = 0; j0 < kmin; j0 += QRB) {
-    const int jn = min(QRB, kmin - j0);
+  for (int j0 = 0; j0 < kmin && j0 / QRB < max_panels; j0 += QRB) {
+    const int jn = min(min(QRB, max_jn), kmin - j0);
     const int mr = m - j0;
     double* Ap = A + j0 + (int64_t)j0 * lda;
     for (int e = threadIdx.x; e < mr * jn; e += blockDim.x) {
@@ -631,6 +632,23 @@ FRANK_D void cta_apply_q_blocked(int m, int k, const double* A, int64_t lda, con
     SUB_MARK(7);
     panel_x_minus_vw(mr, jn, smP, mr, W, r, Xp, ldx);
     SUB_MARK(8);
+  }
+}
+
+// T factors (dlarft, forward / columnwise) of the first k Householder
+// reflectors stored below the diagonal of A (m rows, lda; tau), panel by panel
+// of QRB columns into Tf + p * QRB * QRB -- the layout cta_apply_q_blocked
+// reads -- for reflectors produced by a column-by-column factorization.
+FRANK_D void cta_form_t(int m, int k, const double* A, int64_t lda, const double* tau, double* Tf, double* smP,
+                        double* smT) {
+  for (int j0 = 0; j0 < k; j0 += QRB) {
+    const int jn = min(QRB, k - j0);
+    const int mr = m - j0;
+    cta_load_v(mr, jn, A + j0 + (int64_t)j0 * lda, lda, smP);
+    cta_larft(mr, jn, smP, tau + j0, smT);
+    double* Tp = Tf + (int64_t)(j0 / QRB) * QRB * QRB;
+    for (int e = threadIdx.x; e < QRB * QRB; e += blockDim.x) Tp[e] = smT[e];
+    __syncthreads();
   }
 }
 
@@ -944,6 +962,162 @@ FRANK_D int cta_truncated_geqp3_blocked(int m, int n, double* A, int64_t lda, do
       if (r >= n) maxc = 0.0;
     }
     if (k == 0) break;
+  }
+  __syncthreads();
+  return r;
+}
+
+
+// ---------------------------------------------------------------------------
+// Truncated column-pivoted QR with randomized block pivoting (Martinsson,
+// Quintana-Orti, Heavner, van de Geijn, "Householder QR factorization with
+// randomization for column pivoting (HQRRP)", SIAM J. Sci. Comput. 39, 2017):
+// per panel of QRB columns, a sketch Y = Omega A_trail (QRB + 8 rows, Omega
+// uniform in [-1, 1) from a counter-based hash) picks the panel's pivots by a
+// pivoted QR of Y, the chosen columns move to the panel, and an unpivoted
+// blocked Householder step factors the panel and updates the trailing matrix
+// with two CTA GEMMs -- instead of one pivot search and one pass over the
+// trailing matrix per column.  The stopping rule is the unblocked one,
+// evaluated exactly: after each panel the norms of every remaining column at
+// every step t of the panel follow from the updated rows (the later
+// reflectors act orthogonally below row t), and the rank is the first step
+// whose remaining columns are all at most thr.  Same outputs as
+// cta_truncated_geqp3 (R and reflectors in A, tau, jpvt); the pivots are a
+// randomized choice, so ranks can differ from the column-by-column search by
+// a few.  Scratch ws (global): 40 (m + n) + 40 + 33 n + 8 n + QRB^2 doubles
+// (rqrcp_scratch); smP / smT / gsm as cta_qr_blocked.  Returns the rank.
+// ---------------------------------------------------------------------------
+FRANK_HD int64_t rqrcp_scratch(int m, int n) {
+  return 40 * ((int64_t)m + n) + 40 + 33 * (int64_t)n + 8 * (int64_t)n + 32 * 32 + 64;
+}
+
+FRANK_D double rqrcp_omega(uint64_t k) {
+  k += 0x9E3779B97F4A7C15ull;
+  k = (k ^ (k >> 30)) * 0xBF58476D1CE4E5B9ull;
+  k = (k ^ (k >> 27)) * 0x94D049BB133111EBull;
+  k ^= k >> 31;
+  return (double)(k >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+template <int NT>
+FRANK_D int cta_rand_qrcp(int m, int n, double* A, int64_t lda, double thr, int maxr, double* tau, int* jpvt,
+                          double* ws, double* smP, double* smT, double* gsm, double* red, int* redi) {
+  constexpr int SBMAX = QRB + 8;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int mind = min(min(m, n), maxr);
+  double* Om = ws;                                   // SBMAX x m
+  double* Y = Om + (int64_t)SBMAX * m;               // SBMAX x n
+  double* tau_s = Y + (int64_t)SBMAX * n;            // SBMAX
+  double* cn_s = tau_s + SBMAX;                      // n
+  double* pn_s = cn_s + n;                           // n
+  double* nrm2 = pn_s + n;                           // n
+  double* Wt = nrm2 + n;                             // QRB x n
+  double* Tf = Wt + (int64_t)QRB * n;                // QRB x QRB
+  int* jp_s = reinterpret_cast<int*>(Tf + QRB * QRB);   // n
+  int* pos = jp_s + n;                               // n
+  int* inv = pos + n;                                // n
+  int* swp = inv + n;                                // QRB
+  for (int c = threadIdx.x; c < n; c += blockDim.x) jpvt[c] = c;
+  // the unblocked rule's first test: every column at most thr
+  double best = 0.0;
+  for (int c = wid; c < n; c += nw) {
+    double s2 = 0.0;
+    for (int e = lane; e < m; e += 32) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
+    s2 = warp_sum(s2);
+    best = fmax(best, s2);
+  }
+  if (lane == 0) red[wid] = best;
+  __syncthreads();
+  best = 0.0;
+  for (int w = 0; w < nw; ++w) best = fmax(best, red[w]);
+  __syncthreads();
+  if (mind == 0 || sqrt(best) <= thr) return 0;
+  int r = 0;
+  int panel = 0;
+  while (r < mind) {
+    const int b = min(QRB, mind - r);
+    const int mr = m - r, nr = n - r;
+    const int sb = min(b + 8, mr);
+    // 1. sketch of the trailing matrix
+    for (int64_t e = threadIdx.x; e < (int64_t)sb * mr; e += blockDim.x)
+      Om[e] = rqrcp_omega(((uint64_t)panel << 40) ^ (uint64_t)e);
+    __syncthreads();
+    cta_gemm<double, NT>(sb, nr, mr, 1.0, Om, sb, false, A + r + (int64_t)r * lda, lda, false, 0.0, Y, sb, gsm);
+    // 2. the panel's pivots: b steps of the pivoted QR of the sketch
+    cta_truncated_geqp3(sb, nr, Y, sb, -1.0, b, tau_s, cn_s, pn_s, jp_s, red, redi);
+    // 3. swaps that bring the chosen columns to r .. r+b-1, then applied row-parallel
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < nr; ++c) { pos[c] = c; inv[c] = c; }
+      for (int t = 0; t < b; ++t) {
+        const int want = jp_s[t], cur = pos[want], o = inv[t];
+        swp[t] = cur;
+        inv[t] = want; inv[cur] = o; pos[want] = t; pos[o] = cur;
+        const int q = jpvt[r + t]; jpvt[r + t] = jpvt[r + cur]; jpvt[r + cur] = q;
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < m; e += blockDim.x)
+      for (int t = 0; t < b; ++t) {
+        const int cur = swp[t];
+        if (cur != t) {
+          double* a0 = A + e + (int64_t)(r + t) * lda;
+          double* a1 = A + e + (int64_t)(r + cur) * lda;
+          const double v = *a0; *a0 = *a1; *a1 = v;
+        }
+      }
+    __syncthreads();
+    // 4. unpivoted Householder panel and its trailing update
+    cta_qr_blocked<NT>(mr, nr, A + r + (int64_t)r * lda, lda, tau + r, Tf, Wt, smP, smT, gsm, red, 1, b);
+    // 5. exact norms of the remaining columns at every step t of the panel:
+    //    panel column j (t <= j < b): sum_{i=t..j} R(r+i, r+j)^2; trailing
+    //    column c: ||A(r+b:, c)||^2 + sum_{i=t..b-1} A(r+i, c)^2
+    for (int c = r + b + wid; c < n; c += nw) {
+      double s2 = 0.0;
+      for (int e = r + b + lane; e < m; e += 32) s2 += A[e + (int64_t)c * lda] * A[e + (int64_t)c * lda];
+      s2 = warp_sum(s2);
+      if (lane == 0) nrm2[c] = s2;
+    }
+    __syncthreads();
+    // maxima over columns per step t, as the bits of non-negative doubles
+    // (ordered like unsigned integers) in gsm
+    unsigned long long* mx = reinterpret_cast<unsigned long long*>(gsm);
+    for (int t = threadIdx.x; t <= QRB; t += blockDim.x) mx[t] = 0ull;
+    __syncthreads();
+    for (int c0 = r + b; c0 < n; c0 += blockDim.x) {
+      const int c = c0 + threadIdx.x;
+      const bool on = c < n;
+      double s2 = on ? nrm2[c] : 0.0;
+      double v = s2;
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (lane == 0) atomicMax(mx + b, (unsigned long long)__double_as_longlong(v));
+      for (int t = b - 1; t >= 0; --t) {
+        if (on) {
+          const double a = A[r + t + (int64_t)c * lda];
+          s2 += a * a;
+        }
+        v = s2;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) atomicMax(mx + t, (unsigned long long)__double_as_longlong(v));
+      }
+    }
+    for (int j = threadIdx.x; j < b; j += blockDim.x) {
+      double s2 = 0.0;
+      for (int t = j; t >= 0; --t) {
+        const double a = A[r + t + (int64_t)(r + j) * lda];
+        s2 += a * a;
+        atomicMax(mx + t, (unsigned long long)__double_as_longlong(s2));
+      }
+    }
+    __syncthreads();
+    // every thread reads the same maxima: the first step whose remaining
+    // columns are all at most thr (b: none in this panel)
+    int stop = -1;
+    for (int t = 0; t <= b; ++t)
+      if (sqrt(__longlong_as_double((long long)mx[t])) <= thr) { stop = t; break; }
+    __syncthreads();
+    if (stop >= 0) return r + stop;
+    r += b;
+    ++panel;
   }
   __syncthreads();
   return r;

@@ -63,7 +63,9 @@ typedef struct frank_blr frank_blr;
 typedef struct frank_blr_desc {
   int64_t n;          /* matrix order */
   int32_t nb;         /* blocks per side; block sizes follow IndexRange::split
-                         (index_range.cpp:15-24): ceil(n/nb), last takes the rest */
+                         (index_range.cpp:15-24): ceil(n/nb), last takes the rest;
+                         ceil(n/nb) <= 810 (the recompression keeps its
+                         Householder panels in shared memory) */
   int32_t max_rank;   /* rank capacity of every low-rank block (0 = block size) */
   int32_t precision;  /* FRANK_PREC_* */
   int32_t fixed_rank; /* >0: recompress to this rank (LowRank fixed-rank mode);

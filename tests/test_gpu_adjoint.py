@@ -57,7 +57,7 @@ def test_adjoint_matches_finite_differences_through_gpu(gpu_lib):
 
     def loss_at(t, grad=False):
         th = torch.tensor(t, dtype=torch.float64, device="cuda", requires_grad=grad)
-        x = solve_exp(b, th, pts, nb, eps=1e-12, nugget=nugget, precision="fp64", tol=1e-14)
+        x = solve_exp(b, th, pts, nb, eps=1e-12, nugget=nugget, precision="fp64", tol=1e-13)
         L = 0.5 * (x * x).sum()
         if grad:
             L.backward()
