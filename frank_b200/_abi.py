@@ -52,6 +52,8 @@ SIGNATURES = {
     "frank_copy": (C.c_int, [_vp, _vp, C.c_size_t, C.c_int]),
     "frank_blr_autotune": (C.c_int, [_vp, C.c_int, _vp]),
     "frank_blr_tuning": (C.c_int, [_vp, _ip, _ip, _ip]),
+    "frank_blr_core_smem": (C.c_int, [_vp, _ip]),
+    "frank_blr_set_core_smem": (C.c_int, [_vp, C.c_int]),
     "frank_blr_set_tuning": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
     "frank_blr_write_json": (C.c_int, [_vp, C.c_int, C.c_char_p]),
     "frank_blr_trsm": (C.c_int, [_vp, C.c_int, _dp, C.c_int64, C.c_int, _vp]),

@@ -230,7 +230,14 @@ class BLRMatrix:
     def tuning(self) -> dict:
         v = [C.c_int() for _ in range(3)]
         check(lib().frank_blr_tuning(self._h, *[C.byref(t) for t in v]), "frank_blr_tuning")
-        return {"band_rows": v[0].value, "split_rank": v[1].value, "projected": bool(v[2].value)}
+        cs = C.c_int()
+        check(lib().frank_blr_core_smem(self._h, C.byref(cs)), "frank_blr_core_smem")
+        return {"band_rows": v[0].value, "split_rank": v[1].value, "projected": bool(v[2].value),
+                "core_smem_doubles": cs.value}
+
+    def set_core_smem(self, doubles: int):
+        """Largest recompression core (doubles) kept in shared memory."""
+        check(lib().frank_blr_set_core_smem(self._h, int(doubles)), "frank_blr_set_core_smem")
 
     def write_json(self, path: str, which: int = 0):
         """The block tree with per-block singular values, in the layout of

@@ -93,6 +93,7 @@ struct frank_blr {
   // launch parameters the autotuner chooses (frank_blr_autotune)
   int dupd_band = DUPD_BAND;     // rows per dense-update task
   int split_p = SPLIT_P;         // split band-1 targets above this operand rank (0: never)
+  int core_smem = RECOMP_REGION; // recompression cores up to this many doubles stay in shared memory
   double core_scale = 0.1;
   int grid_gram = 0;
   double gram_tol = 1e-12;
@@ -376,14 +377,15 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
         ++launches;
         if (p->dense_offdiag) {
           k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
-              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr, 0, 0);
+              W, ws, i, p->smax, p->core_method, p->core_scale, 1, p->work + p->nb + i, 0, nullptr, nullptr, 0, 0,
+              p->core_smem);
           ++launches;
         }
       } else {
         k_recompress<T><<<std::min(mm, p->grid_recomp), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(
             W, ws, i, p->smax, p->fixed_rank > 0 ? p->core_fixed : p->core_method, p->core_scale, 0, p->work + i,
             p->rsplit ? p->nsplit : 0, p->rsplit, p->split_done ? p->split_done + (size_t)i * SPLIT_MAX : nullptr,
-            p->proj_tol ? 1 : 0, p->split_p);
+            p->proj_tol ? 1 : 0, p->split_p, p->core_smem);
         ++launches;
       }
     }
@@ -1399,7 +1401,7 @@ struct TuneKey {
   }
 };
 struct TuneVal {
-  int band, split, proj;
+  int band, split, proj, core_smem;
   double ms;
 };
 std::map<TuneKey, TuneVal> g_tuned;
@@ -1453,6 +1455,7 @@ int frank_blr_autotune(frank_blr* p, int force, void* stream) {
       p->dupd_band = it->second.band;
       p->split_p = it->second.split;
       p->proj_tol = it->second.proj != 0;
+      p->core_smem = it->second.core_smem;
       drop_graph(p);
       return FRANK_OK;
     }
@@ -1489,9 +1492,12 @@ int frank_blr_autotune(frank_blr* p, int force, void* stream) {
     if (t < best) { best = t; proj = !keep; }
     p->proj_tol = proj != 0;
   }
+  // largest recompression core kept in shared memory: larger ones take the
+  // blocked / randomized paths in L2 (randomized pivoting for the RRQR core)
+  if (p->nlr > 0 && (rc = try_values(&p->core_smem, {RECOMP_REGION, 16384, 6144}))) return rc;
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tuned[key] = TuneVal{p->dupd_band, p->split_p, p->proj_tol ? 1 : 0, best};
+    g_tuned[key] = TuneVal{p->dupd_band, p->split_p, p->proj_tol ? 1 : 0, p->core_smem, best};
   }
   drop_graph(p);
   return FRANK_OK;
@@ -1511,6 +1517,19 @@ int frank_blr_tuning(const frank_blr* p, int* band_rows, int* split_rank, int* p
   if (band_rows) *band_rows = p->dupd_band;
   if (split_rank) *split_rank = p->split_p;
   if (projected) *projected = p->proj_tol ? 1 : 0;
+  return FRANK_OK;
+}
+
+int frank_blr_core_smem(const frank_blr* p, int* doubles) {
+  if (!p || !doubles) return fail(FRANK_ERR_INVALID, "null argument");
+  *doubles = p->core_smem;
+  return FRANK_OK;
+}
+
+int frank_blr_set_core_smem(frank_blr* p, int doubles) {
+  if (!p || doubles < 1) return fail(FRANK_ERR_INVALID, "bad core size");
+  p->core_smem = doubles;
+  drop_graph(p);
   return FRANK_OK;
 }
 

@@ -1128,7 +1128,7 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
                                                                int core_method, double core_scale,
                                                                int only_dense_operands, int* counter, int nsplit,
                                                                double* split_base, int* split_done, int proj_tol,
-                                                               int split_p) {
+                                                               int split_p, int core_smem) {
   extern __shared__ double dsm[];
   double* gsm = dsm;
   double* region = dsm + RECOMP_GSM;
@@ -1287,7 +1287,10 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     cta_gemm<double, RECOMP_THREADS>(mu, o.q, o.p, 1.0, Rc + (int64_t)kc * mu, mu, false, Tm, o.p, false, 0.0,
                                      Mtmp + (int64_t)kc * mu, mu, gsm);
     // core M (mu x mv) = Mtmp Rv^T, in shared memory if it fits
-    const bool in_smem = (int64_t)mu * mv + 4 * (int64_t)mv + 2 * mu <= RECOMP_REGION;
+    // the core in shared memory when it fits and is not above the tuned size
+    // (small cores always: the L2 paths need mu >= 64 for their T scratch)
+    const int64_t core_need = (int64_t)mu * mv + 4 * (int64_t)mv + 2 * mu;
+    const bool in_smem = core_need <= RECOMP_REGION && (mu < 64 || core_need <= core_smem);
     double* Mm = in_smem ? region : Mg;
     cta_gemm<double, RECOMP_THREADS>(mu, mv, sv, 1.0, Mtmp, mu, false, Rv, mv, true, 0.0, Mm, mu, gsm);
     PHASE_MARK(cls, 3);

@@ -295,6 +295,12 @@ int frank_blr_set_tuning(frank_blr* plan, int band_rows, int split_rank, int pro
 /* The plan's current launch parameters (see frank_blr_autotune). */
 int frank_blr_tuning(const frank_blr* plan, int* band_rows, int* split_rank, int* projected);
 
+/* The largest recompression core (in doubles) kept in shared memory; larger
+ * cores take the L2 paths (randomized block pivoting for the RRQR core,
+ * blocked WY).  Chosen by frank_blr_autotune; 0 < value.  */
+int frank_blr_core_smem(const frank_blr* plan, int* doubles);
+int frank_blr_set_core_smem(frank_blr* plan, int doubles);
+
 /* Counters of the last getrf: kernels launched by it plus those of every
  * solve / matvec / refine since, recompressions performed, the largest
  * recompressed rank and the number of ranks clamped at max_rank. */
