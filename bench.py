@@ -520,11 +520,11 @@ def run_ours_sample(stream, steps):
 # DRAM traffic of k_recompress per algorithmic FLOP, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum over all 15 recompression
 # launches of `--profile-case n8192`, the mixed factor at the headline's
-# tolerance: 1.610e9 bytes for 5.454e10 FLOPs; the workload is too large to
+# tolerance: 1.616e9 bytes for 4.695e10 FLOPs; the workload is too large to
 # capture whole).  The roofline's `traffic` scales it to the mean headline
 # launch by the FLOPs that launch performs
 # (profiles/k_recompress_blr_laplace3d_n8192.md).
-RECOMP_BYTES_PER_FLOP = 1.610e9 / 5.454e10
+RECOMP_BYTES_PER_FLOP = 1.616e9 / 4.695e10
 
 
 def profile_case(name):
