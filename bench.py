@@ -601,17 +601,19 @@ def workload_batched(args):
     xp = [X[k].data_ptr() for k in range(count)]
     for _ in range(args.warmup):
         batch.getrf(); batch.refine_device(bp, xp, nmax, 1, tol=1e-10)
-    times = []
+    times, tg = [], []
     for _ in range(args.steps):
         torch.cuda.synchronize(); t0 = time.perf_counter()
         batch.getrf()
+        torch.cuda.synchronize(); t1 = time.perf_counter()
         its, res = batch.refine_device(bp, xp, nmax, 1, tol=1e-10)
-        torch.cuda.synchronize(); times.append(time.perf_counter() - t0)
+        torch.cuda.synchronize(); times.append(time.perf_counter() - t0); tg.append(t1 - t0)
     t = statistics.median(times)
     ranks = [p.rank(i, j, 1) for p in plans[:8] for i in range(p.nb) for j in range(p.nb) if i != j]
     print(json.dumps({"workload": "batched: 256 systems N in {1024..8192}, -log kernel + N I, b=256, eps 1e-6",
                       "value": t, "unit": "s", "systems_per_s": count / t, "systems": count,
                       "total_unknowns": int(sizes.sum()), "max_iters": int(max(its)), "max_residual": max(res),
+                      "getrf_s": statistics.median(tg), "refine_s": t - statistics.median(tg),
                       "mean_rank_first8": float(np.mean(ranks)), "build_s": t_build,
                       "steps": args.steps, "warmup": args.warmup}), flush=True)
 

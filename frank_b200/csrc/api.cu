@@ -349,7 +349,8 @@ int enqueue_factor(frank_blr* p, cudaStream_t s, bool timing = true) {
       const int band = std::min(p->dupd_band, p->bmax);
       const int nbands = (p->bmax + band - 1) / band;
       if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 0), sd, cudaEventRecordExternal));
-      k_update_dense<T><<<nbands, DUPD_THREADS, 0, sd>>>(W, ws, i, p->dupd_band, DUPD_NEXT);
+      // one task per band; its CTA index picks a scratch slot (grid_dense of them)
+      k_update_dense<T><<<std::min(nbands, p->grid_dense), DUPD_THREADS, 0, sd>>>(W, ws, i, p->dupd_band, DUPD_NEXT);
       if (timing) CUDA_TRY(cudaEventRecordWithFlags(ev_at(p, i, EV_DENSE_NEXT, 1), sd, cudaEventRecordExternal));
       ++launches;
       if (sd == s) {
@@ -879,6 +880,10 @@ int create_impl(const frank_blr_desc* d, const double* points, int dim, frank_bl
   cudaFuncSetAttribute(k_trinv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRINV_SMEM_MAX);
   cudaFuncSetAttribute(k_recompress<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
+  cudaFuncSetAttribute(k_recompress_b<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
+  cudaFuncSetAttribute(k_recompress_b<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, RECOMP_SMEM_BYTES);
+  cudaFuncSetAttribute(k_trinv_b<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRINV_SMEM_MAX);
+  cudaFuncSetAttribute(k_trinv_b<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRINV_SMEM_MAX);
   cudaFuncSetAttribute(k_recompress_gram<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, GRAM_SMEM_BYTES);
   cudaFuncSetAttribute(k_recompress_gram<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, GRAM_SMEM_BYTES);
   *out = p;
@@ -1618,6 +1623,13 @@ struct frank_batch {
   std::vector<cudaEvent_t> join;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // one launch per elimination step over all systems (when they share the
+  // block size and launch grids): the device table of the systems and the
+  // step events of the two streams
+  bool stepwise = false;
+  void* d_sys = nullptr;
+  cudaStream_t aux = nullptr;
+  std::vector<cudaEvent_t> ev_getrf, ev_panel, ev_dense;
 };
 
 namespace {
@@ -1625,6 +1637,10 @@ void free_batch(frank_batch* B) {
   if (!B) return;
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
+  if (B->d_sys) cudaFree(B->d_sys);
+  if (B->aux) cudaStreamDestroy(B->aux);
+  for (auto* v : {&B->ev_getrf, &B->ev_panel, &B->ev_dense})
+    for (auto e : *v) if (e) cudaEventDestroy(e);
   for (auto e : B->join) if (e) cudaEventDestroy(e);
   if (B->fork) cudaEventDestroy(B->fork);
   for (auto st : B->streams) if (st) cudaStreamDestroy(st);
@@ -1687,12 +1703,169 @@ extern "C" int frank_batch_destroy(frank_batch* B) {
 }
 
 namespace {
+// A batch factors step by step (one launch per elimination step over all
+// systems) when its plans share the block size (every block full), the
+// launch grids and the dense-update band, and use the Householder
+// recompression; otherwise each system is its own branch of one graph.
+bool batch_stepwise_ok(const frank_batch* B) {
+  const frank_blr* q = B->plans[0];
+  for (const frank_blr* p : B->plans) {
+    if (p->bmax != q->bmax || p->n != (int64_t)p->nb * p->bmax || use_gram(p) || p->grid_recomp != q->grid_recomp ||
+        p->grid_dense != q->grid_dense || p->grid_gram != q->grid_gram || p->dupd_band != q->dupd_band)
+      return false;
+  }
+  return true;
+}
+
+// The step-by-step schedule of enqueue_factor over all systems of a batch:
+// the same two streams and events, each launch with grid.z = systems.
+// Device table of the systems, step events and the second stream (before
+// the capture: allocations and copies are not captured).
+template <typename T>
+int prepare_stepwise(frank_batch* B) {
+  const int K = (int)B->plans.size();
+  int max_nb = 0;
+  // systems in decreasing order of their number of steps: the systems that
+  // still have a step i are then a prefix of the table, and each launch covers
+  // only them (grid.z), the largest first in the block scheduling order
+  std::vector<int> order(K);
+  for (int k = 0; k < K; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return B->plans[a]->nb > B->plans[c]->nb; });
+  std::vector<SysDev<T>> sys(K);
+  for (int k = 0; k < K; ++k) {
+    frank_blr* p = B->plans[order[k]];
+    max_nb = std::max(max_nb, p->nb);
+    SysDev<T>& d = sys[k];
+    d.H = h_view(p);
+    d.W = work_view<T>(p);
+    d.ws = factor_ws<T>(p);
+    d.work = p->work;
+    d.rscratch = p->rscratch;
+    d.rstride = p->rstride;
+    d.core_scale = p->core_scale;
+    d.thr_trunc = p->core_scale * p->eps;
+    d.smax = p->smax;
+    d.core_method = p->fixed_rank > 0 ? p->core_fixed : p->core_method;
+    d.proj_tol = p->proj_tol ? 1 : 0;
+    d.split_p = p->split_p;
+    d.core_smem = p->core_smem;
+    d.dupd_band = p->dupd_band;
+    d.pretrunc = pretruncate(p) ? 1 : 0;
+    d.has_lr = p->nlr > 0 ? 1 : 0;
+  }
+  if (!B->d_sys) CUDA_TRY(cudaMalloc(&B->d_sys, sizeof(SysDev<T>) * K));
+  CUDA_TRY(cudaMemcpy(B->d_sys, sys.data(), sizeof(SysDev<T>) * K, cudaMemcpyHostToDevice));
+  if ((int)B->ev_getrf.size() < max_nb) {
+    for (auto* v : {&B->ev_getrf, &B->ev_panel, &B->ev_dense}) {
+      const size_t old = v->size();
+      v->resize(max_nb, nullptr);
+      for (size_t e = old; e < v->size(); ++e)
+        CUDA_TRY(cudaEventCreateWithFlags(&(*v)[e], cudaEventDisableTiming));
+    }
+  }
+  if (!B->aux) CUDA_TRY(cudaStreamCreateWithFlags(&B->aux, cudaStreamNonBlocking));
+  return FRANK_OK;
+}
+
+template <typename T>
+int enqueue_factor_stepwise(frank_batch* B, cudaStream_t s) {
+  const int K = (int)B->plans.size();
+  frank_blr* q = B->plans[0];
+  int max_nb = 0;
+  bool any_trunc = false;
+  for (frank_blr* p : B->plans) {
+    max_nb = std::max(max_nb, p->nb);
+    any_trunc = any_trunc || pretruncate(p);
+  }
+  const SysDev<T>* S = static_cast<const SysDev<T>*>(B->d_sys);
+  // systems with a step i: a prefix of the table (ordered by decreasing nb)
+  std::vector<int> nbs;
+  for (frank_blr* p : B->plans) nbs.push_back(p->nb);
+  auto active = [&](int i) {
+    int c = 0;
+    for (int v : nbs) c += v > i;
+    return std::max(c, 1);
+  };
+  cudaStream_t s2 = B->aux;
+  const int b = q->bmax;
+  const int cw = trinv_width(b);
+  const int rt = (b + PANEL_TILE - 1) / PANEL_TILE;
+  const int band = std::min(q->dupd_band, b);
+  const int nbands = (b + band - 1) / band;
+  k_reset_b<T><<<dim3(max_nb * max_nb, 1, K), 256, 0, s>>>(S);
+  for (frank_blr* p : B->plans) {
+    CUDA_TRY(cudaMemsetAsync(p->err, 0, ERR_SLOTS * sizeof(int), s));
+    CUDA_TRY(cudaMemsetAsync(p->flops, 0, FLOP_SLOTS * sizeof(unsigned long long), s));
+    CUDA_TRY(cudaMemsetAsync(p->work, 0, 2 * p->nb * sizeof(int), s));
+  }
+  CUDA_TRY(cudaEventRecord(B->fork, s));
+  CUDA_TRY(cudaStreamWaitEvent(s2, B->fork, 0));
+  if (any_trunc)
+    k_truncate_lr_b<T><<<dim3(std::max(q->grid_recomp, q->grid_gram), 1, K), TRUNC_THREADS, 0, s>>>(S);
+  auto getrf_step = [&](int step) -> int {
+    const int Kz = active(step);
+    k_getrf_load_b<T><<<dim3(64, 1, Kz), GETRF_AUX_THREADS, 0, s2>>>(S, step);
+    for (int jb = 0; jb < b; jb += 32) {
+      k_getrf_panel_b<T><<<dim3(1, 1, Kz), GETRF_THREADS, 0, s2>>>(S, step, jb);
+      const int m2 = b - jb - std::min(32, b - jb);
+      if (m2 > 0) {
+        const int nt = (m2 + 63) / 64;
+        k_getrf_trail_b<T><<<dim3(nt * nt, 1, Kz), GETRF_AUX_THREADS, 0, s2>>>(S, step, jb);
+      }
+    }
+    k_getrf_store_b<T><<<dim3(64, 1, Kz), GETRF_AUX_THREADS, 0, s2>>>(S, step);
+    k_trinv_b<T><<<dim3(2 * ((b + cw - 1) / cw), 1, Kz), TRINV_THREADS, (size_t)b * cw * sizeof(double), s2>>>(
+        S, step, cw);
+    CUDA_TRY(cudaEventRecord(B->ev_getrf[step], s2));
+    return FRANK_OK;
+  };
+  int rc = getrf_step(0);
+  if (rc) return rc;
+  for (int i = 0; i < max_nb; ++i) {
+    CUDA_TRY(cudaStreamWaitEvent(s, B->ev_getrf[i], 0));
+    const int m = max_nb - i - 1;
+    if (m == 0) break;
+    const int Kz = active(i + 1);   // systems with targets at step i (nb > i + 1)
+    k_panel_gather_b<T><<<dim3(m, rt, Kz), PANEL_THREADS, 0, s>>>(S, i);
+    k_panel_mul_b<T><<<dim3(2 * m, rt, Kz), PANEL_THREADS, 0, s>>>(S, i);
+    k_panel_fin_b<T><<<dim3(2 * m, rt, Kz), PANEL_THREADS, 0, s>>>(S, i);
+    CUDA_TRY(cudaEventRecord(B->ev_panel[i], s));
+    CUDA_TRY(cudaStreamWaitEvent(s2, B->ev_panel[i], 0));
+    k_update_dense_b<T><<<dim3(std::min(nbands, q->grid_dense), 1, Kz), DUPD_THREADS, 0, s2>>>(S, i, DUPD_NEXT);
+    if ((rc = getrf_step(i + 1))) return rc;
+    if (m > 1)
+      k_update_dense_b<T><<<dim3((int)std::min<int64_t>((int64_t)m * m * nbands, q->grid_dense), 1, Kz), DUPD_THREADS,
+                            0, s2>>>(S, i, DUPD_REST);
+    CUDA_TRY(cudaEventRecord(B->ev_dense[i], s2));
+    k_recompress_b<T><<<dim3(std::min(m * m, q->grid_recomp), 1, Kz), RECOMP_THREADS, RECOMP_SMEM_BYTES, s>>>(S, i);
+    CUDA_TRY(cudaStreamWaitEvent(s, B->ev_dense[i], 0));
+  }
+  CUDA_TRY(cudaStreamWaitEvent(s, B->ev_getrf[max_nb - 1], 0));
+  CUDA_TRY(cudaGetLastError());
+  for (frank_blr* p : B->plans) { p->timed = false; p->launches = 0; }
+  return FRANK_OK;
+}
+
 template <typename T>
 int batch_capture(frank_batch* B) {
   cudaStream_t s = B->stream;
   for (frank_blr* p : B->plans) {
     int rc0 = ensure_scratch(p);
     if (rc0) return rc0;
+  }
+  B->stepwise = batch_stepwise_ok(B);
+  if (B->stepwise) {
+    int rc0 = prepare_stepwise<T>(B);
+    if (rc0) return rc0;
+    CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_factor_stepwise<T>(B, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc != FRANK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(FRANK_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+    B->graph = g;
+    CUDA_TRY(cudaGraphInstantiate(&B->exec, g, 0));
+    return FRANK_OK;
   }
   CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int rc = FRANK_OK;

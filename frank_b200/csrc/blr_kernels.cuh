@@ -132,7 +132,7 @@ FRANK_HD double fast_rounded_addition_flops(double m, double n, double bi, doubl
 // One CTA per block.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_reset(BlrView<double> H, BlrView<T> W) {
+FRANK_D void k_reset_impl(BlrView<double> H, BlrView<T> W) {
   const int blk = blockIdx.x;
   const int i = blk / H.nb, j = blk % H.nb;
   const int bi = H.bs(i), bj = H.bs(j);
@@ -161,6 +161,11 @@ __global__ void k_reset(BlrView<double> H, BlrView<T> W) {
       wd[rr + (int64_t)c * W.bmax] = T(hd[rr + (int64_t)c * H.bmax]);
     }
   }
+}
+
+template <typename T>
+__global__ void k_reset(BlrView<double> H, BlrView<T> W) {
+  k_reset_impl<T>(H, W);
 }
 
 // ---------------------------------------------------------------------------
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(ORTH_THREADS) k_orthonormalize_lr(BlrView<doub
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr(BlrView<double> H, BlrView<T> W, FactorWs<T> ws,
+FRANK_D void k_truncate_lr_impl(BlrView<double> H, BlrView<T> W, FactorWs<T> ws,
                                                               double thr_scale, double* scratch, int64_t stride) {
   __shared__ double gsm[2 * 16 * 64];
   __shared__ double red[32];
@@ -307,6 +312,12 @@ __global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr(BlrView<double> H
     if (threadIdx.x == 0) W.rank[blk] = r;
     __syncthreads();
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr(BlrView<double> H, BlrView<T> W, FactorWs<T> ws,
+                                                              double thr_scale, double* scratch, int64_t stride) {
+  k_truncate_lr_impl<T>(H, W, ws, thr_scale, scratch, stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -525,7 +536,7 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf(BlrView<T> A, FactorWs<
 constexpr int GETRF_AUX_THREADS = 256;
 
 template <typename T>
-__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_load(BlrView<T> A, FactorWs<T> ws, int i) {
+FRANK_D void k_getrf_load_impl(BlrView<T> A, FactorWs<T> ws, int i) {
   const int b = A.bs(i), ld = A.bmax;
   const T* Dp = A.dense(i, i);
   double* Wm = ws.getrf_scratch;
@@ -537,7 +548,12 @@ __global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_load(BlrView<T> A, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(GETRF_THREADS) k_getrf_panel(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_load(BlrView<T> A, FactorWs<T> ws, int i) {
+  k_getrf_load_impl<T>(A, ws, i);
+}
+
+template <typename T>
+FRANK_D void k_getrf_panel_impl(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
   __shared__ double red[32];
   __shared__ int redi[32];
   __shared__ double gsm[2 * 16 * 64];
@@ -554,7 +570,12 @@ __global__ void __launch_bounds__(GETRF_THREADS) k_getrf_panel(BlrView<T> A, Fac
 }
 
 template <typename T>
-__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_trail(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
+__global__ void __launch_bounds__(GETRF_THREADS) k_getrf_panel(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
+  k_getrf_panel_impl<T>(A, ws, i, jb);
+}
+
+template <typename T>
+FRANK_D void k_getrf_trail_impl(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
   __shared__ double gsm[2 * 16 * 64];
   const int b = A.bs(i);
   if (jb >= b) return;
@@ -572,7 +593,12 @@ __global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_trail(BlrView<T> A,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_store(BlrView<T> A, FactorWs<T> ws, int i) {
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_trail(BlrView<T> A, FactorWs<T> ws, int i, int jb) {
+  k_getrf_trail_impl<T>(A, ws, i, jb);
+}
+
+template <typename T>
+FRANK_D void k_getrf_store_impl(BlrView<T> A, FactorWs<T> ws, int i) {
   const int b = A.bs(i), ld = A.bmax;
   T* Dp = A.dense(i, i);
   const double* Wm = ws.getrf_scratch;
@@ -592,6 +618,11 @@ __global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_store(BlrView<T> A,
     const int r = e % b, c = e / b;
     Dp[r + (int64_t)c * ld] = T(Wm[r + (int64_t)c * b]);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_store(BlrView<T> A, FactorWs<T> ws, int i) {
+  k_getrf_store_impl<T>(A, ws, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -615,7 +646,7 @@ inline int trinv_width(int bmax) { return bmax <= 640 ? 32 : 16; }
 constexpr int TRINV_SMEM_MAX = 640 * 32 * (int)sizeof(double);   // covers 1024 x 16 too
 
 template <typename T>
-__global__ void __launch_bounds__(TRINV_THREADS) k_trinv(BlrView<T> A, FactorWs<T> ws, int i, int cw) {
+FRANK_D void k_trinv_impl(BlrView<T> A, FactorWs<T> ws, int i, int cw) {
   extern __shared__ double X[];        // b x cw (ld b), rows indexed absolutely
   __shared__ double tri[32 * 33];
   __shared__ double acc[32 * 32];
@@ -683,6 +714,11 @@ __global__ void __launch_bounds__(TRINV_THREADS) k_trinv(BlrView<T> A, FactorWs<
     atomicAdd(ws.flops + FLOP_GETRF, (unsigned long long)(2.0 / 3.0 * (double)b * b * b));
 }
 
+template <typename T>
+__global__ void __launch_bounds__(TRINV_THREADS) k_trinv(BlrView<T> A, FactorWs<T> ws, int i, int cw) {
+  k_trinv_impl<T>(A, ws, i, cw);
+}
+
 // ---------------------------------------------------------------------------
 // K2: panel of step i (trsm.cpp:92-115 with the leaf inverse; the pivots of
 // K1 applied).  Task t < m: column-panel block (i+1+t, i):
@@ -744,7 +780,7 @@ FRANK_D T* panel_data(const BlrView<T>& A, const PanelTask<T>& P) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(PANEL_THREADS) k_panel_gather(BlrView<T> A, FactorWs<T> ws, int i) {
+FRANK_D void k_panel_gather_impl(BlrView<T> A, FactorWs<T> ws, int i) {
   const int m = A.nb - i - 1;
   const PanelTask<T> P = panel_task(A, ws, i, m + blockIdx.x);
   const int r0 = blockIdx.y * PANEL_TILE;
@@ -759,7 +795,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_gather(BlrView<T> A, Fa
 }
 
 template <typename T>
-__global__ void __launch_bounds__(PANEL_THREADS) k_panel_mul(BlrView<T> A, FactorWs<T> ws, int i) {
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_gather(BlrView<T> A, FactorWs<T> ws, int i) {
+  k_panel_gather_impl<T>(A, ws, i);
+}
+
+template <typename T>
+FRANK_D void k_panel_mul_impl(BlrView<T> A, FactorWs<T> ws, int i) {
   __shared__ T gsm[2 * 16 * 64];
   const int t = blockIdx.x;
   const PanelTask<T> P = panel_task(A, ws, i, t);
@@ -786,7 +827,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_mul(BlrView<T> A, Facto
 }
 
 template <typename T>
-__global__ void __launch_bounds__(PANEL_THREADS) k_panel_fin(BlrView<T> A, FactorWs<T> ws, int i) {
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_mul(BlrView<T> A, FactorWs<T> ws, int i) {
+  k_panel_mul_impl<T>(A, ws, i);
+}
+
+template <typename T>
+FRANK_D void k_panel_fin_impl(BlrView<T> A, FactorWs<T> ws, int i) {
   __shared__ T gsm[2 * 16 * 64];
   const int t = blockIdx.x;
   const PanelTask<T> P = panel_task(A, ws, i, t);
@@ -809,6 +855,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_fin(BlrView<T> A, Facto
     cta_gemm<T, PANEL_THREADS>(rn, P.r, P.r, T(1), d + r0, ld, false, A.s(bi_, bj_), A.kcap, false, T(0),
                                P.tmp + r0, ld, gsm);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_fin(BlrView<T> A, FactorWs<T> ws, int i) {
+  k_panel_fin_impl<T>(A, ws, i);
 }
 
 // Task t (0 <= t < m*(m-1)) of step i's off-diagonal targets, ordered by
@@ -899,7 +950,7 @@ constexpr int DUPD_BAND = 128;    // rows of a dense update task (default; the a
 enum DenseUpdateMode { DUPD_ALL = 0, DUPD_NEXT = 1, DUPD_REST = 2 };
 
 template <typename T>
-__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i, int band_rows,
+FRANK_D void k_update_dense_impl(BlrView<T> A, FactorWs<T> ws, int i, int band_rows,
                                                                 int mode) {
   __shared__ double gsm[2 * 16 * 64];
   __shared__ T gsmt[2 * 16 * 64];
@@ -942,6 +993,12 @@ __global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, Fac
     else
       cta_gemm<T, DUPD_THREADS>(rn, bk, o.q, T(1), X, ldx, false, o.YR, ld, false, T(1), C, ld, gsmt);
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense(BlrView<T> A, FactorWs<T> ws, int i, int band_rows,
+                                                                int mode) {
+  k_update_dense_impl<T>(A, ws, i, band_rows, mode);
 }
 
 // ---------------------------------------------------------------------------
@@ -1124,7 +1181,7 @@ FRANK_HD RecompLayout recomp_layout(int bmax, int smax) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
+FRANK_D void k_recompress_impl(BlrView<T> A, FactorWs<T> ws, int i, int smax,
                                                                int core_method, double core_scale,
                                                                int only_dense_operands, int* counter, int nsplit,
                                                                double* split_base, int* split_done, int proj_tol,
@@ -1453,6 +1510,15 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
     }
 #endif
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, FactorWs<T> ws, int i, int smax,
+                                                               int core_method, double core_scale,
+                                                               int only_dense_operands, int* counter, int nsplit,
+                                                               double* split_base, int* split_done, int proj_tol,
+                                                               int split_p, int core_smem) {
+  k_recompress_impl<T>(A, ws, i, smax, core_method, core_scale, only_dense_operands, counter, nsplit, split_base, split_done, proj_tol, split_p, core_smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -2661,6 +2727,114 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_build_lowrank_rsvd(BlrView<do
     if (threadIdx.x == 0) H.rank[blk] = rk;
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Batched factorization of independent systems: one launch per elimination
+// step covers every system of a batch (grid.z = system).  Each CTA reads its
+// system's views and parameters from a device table and leaves at once when
+// its system has no step i or fewer tasks than its block index; the bodies
+// are the single-system kernels' own.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct SysDev {
+  BlrView<double> H;
+  BlrView<T> W;
+  FactorWs<T> ws;
+  int* work;              // recompression task counters of the system ([nb])
+  double* rscratch;       // reset-truncation scratch (k_truncate_lr)
+  int64_t rstride;
+  double core_scale, thr_trunc;
+  int smax, core_method, proj_tol, split_p, core_smem, dupd_band, pretrunc, has_lr;
+};
+
+template <typename T>
+__global__ void k_reset_b(const SysDev<T>* S) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if ((int)blockIdx.x >= s.H.nb * s.H.nb) return;
+  k_reset_impl<T>(s.H, s.W);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TRUNC_THREADS) k_truncate_lr_b(const SysDev<T>* S) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (!s.pretrunc) return;
+  k_truncate_lr_impl<T>(s.H, s.W, s.ws, s.thr_trunc, s.rscratch, s.rstride);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_load_b(const SysDev<T>* S, int i) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb) return;
+  k_getrf_load_impl<T>(s.W, s.ws, i);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_THREADS) k_getrf_panel_b(const SysDev<T>* S, int i, int jb) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb || jb >= s.W.bs(i)) return;
+  k_getrf_panel_impl<T>(s.W, s.ws, i, jb);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_trail_b(const SysDev<T>* S, int i, int jb) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb) return;
+  const int b = s.W.bs(i);
+  const int m2 = b - jb - min(32, b - jb);
+  const int nt = (m2 + 63) / 64;
+  if (m2 <= 0 || (int)blockIdx.x >= nt * nt) return;
+  k_getrf_trail_impl<T>(s.W, s.ws, i, jb);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GETRF_AUX_THREADS) k_getrf_store_b(const SysDev<T>* S, int i) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb) return;
+  k_getrf_store_impl<T>(s.W, s.ws, i);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TRINV_THREADS) k_trinv_b(const SysDev<T>* S, int i, int cw) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb || (int)blockIdx.x >= 2 * ((s.W.bs(i) + cw - 1) / cw)) return;
+  k_trinv_impl<T>(s.W, s.ws, i, cw);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_gather_b(const SysDev<T>* S, int i) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if ((int)blockIdx.x >= s.W.nb - i - 1) return;
+  k_panel_gather_impl<T>(s.W, s.ws, i);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_mul_b(const SysDev<T>* S, int i) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if ((int)blockIdx.x >= 2 * (s.W.nb - i - 1)) return;
+  k_panel_mul_impl<T>(s.W, s.ws, i);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_fin_b(const SysDev<T>* S, int i) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if ((int)blockIdx.x >= 2 * (s.W.nb - i - 1)) return;
+  k_panel_fin_impl<T>(s.W, s.ws, i);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DUPD_THREADS) k_update_dense_b(const SysDev<T>* S, int i, int mode) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb - 1) return;
+  k_update_dense_impl<T>(s.W, s.ws, i, s.dupd_band, mode);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RECOMP_THREADS) k_recompress_b(const SysDev<T>* S, int i) {
+  const SysDev<T>& s = S[blockIdx.z];
+  if (i >= s.W.nb - 1 || !s.has_lr) return;
+  k_recompress_impl<T>(s.W, s.ws, i, s.smax, s.core_method, s.core_scale, 0, s.work + i, 0, nullptr, nullptr,
+                       s.proj_tol, s.split_p, s.core_smem);
 }
 
 }  // namespace frank
