@@ -591,7 +591,7 @@ def workload_batched(args):
         plans.append(M)
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t0
-    batch = BLRBatch(plans, grid=4)
+    batch = BLRBatch(plans, grid=args.batch_grid)
     rb = np.random.default_rng(3)
     B = torch.zeros((count, nmax), dtype=torch.float64, device="cuda")
     for k, n in enumerate(sizes):
@@ -667,6 +667,8 @@ def main():
     ap.add_argument("--workload", default="headline", choices=["headline", "batched", "adjoint"],
                     help="headline (the bench line); batched / adjoint print their own JSON line")
     ap.add_argument("--systems", type=int, default=256)
+    ap.add_argument("--batch-grid", type=int, default=16,
+                    help="batched workload: CTAs per system of the persistent kernels")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)

@@ -1518,7 +1518,8 @@ __global__ void __launch_bounds__(RECOMP_THREADS) k_recompress(BlrView<T> A, Fac
                                                                int only_dense_operands, int* counter, int nsplit,
                                                                double* split_base, int* split_done, int proj_tol,
                                                                int split_p, int core_smem) {
-  k_recompress_impl<T>(A, ws, i, smax, core_method, core_scale, only_dense_operands, counter, nsplit, split_base, split_done, proj_tol, split_p, core_smem);
+  k_recompress_impl<T>(A, ws, i, smax, core_method, core_scale, only_dense_operands, counter, nsplit, split_base,
+                       split_done, proj_tol, split_p, core_smem);
 }
 
 // ---------------------------------------------------------------------------
