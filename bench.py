@@ -661,11 +661,55 @@ def workload_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def workload_hlu(args):
+    """Multi-level H-LU: Laplace-3D 1/(r+1e-3) on N = 131072 (--hlu-n)
+    Morton-ordered unit-cube points (seed 7), binary cluster tree with weak
+    admissibility, leaves of 256, every off-diagonal block rank 32 (rsvd),
+    FP64 factor, FP64 refinement of 8 RHS (seed 8) against A_H to 1e-10.  A
+    step is getrf + refine; construction is timed apart.  Prints one JSON
+    line."""
+    import torch
+    from frank_b200 import HMatrix
+    n, leaf, rank, nrhs = args.hlu_n, 256, 32, 8
+    pts = make_points(n, 3, 7, 10)
+    M = HMatrix(n, leaf, rank)
+    torch.cuda.synchronize(); t0 = time.perf_counter()
+    M.build_kernel("laplace", pts)
+    torch.cuda.synchronize(); t_build = time.perf_counter() - t0
+    # column-major n x nrhs: the transpose of a contiguous nrhs x n tensor
+    b = torch.tensor(MT19937_64(8).normal(n * nrhs).reshape(nrhs, n), device="cuda").t()
+    X = torch.zeros((nrhs, n), dtype=torch.float64, device="cuda").t()
+    its = res = None
+    for _ in range(args.warmup):
+        M.getrf(); M.refine_device(b.data_ptr(), X.data_ptr(), nrhs, tol=1e-10, maxit=50)
+    times, tf = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize(); t0 = time.perf_counter()
+        M.getrf()
+        torch.cuda.synchronize(); t1 = time.perf_counter()
+        its, res = M.refine_device(b.data_ptr(), X.data_ptr(), nrhs, tol=1e-10, maxit=50)
+        torch.cuda.synchronize(); times.append(time.perf_counter() - t0); tf.append(t1 - t0)
+    # achieved residual, recomputed from the solution
+    Y = torch.zeros_like(X)
+    M.matvec_device(X.data_ptr(), Y.data_ptr(), nrhs)
+    rel = ((b - Y).norm(dim=0) / b.norm(dim=0)).max().item()
+    st = M.stats()
+    print(json.dumps({"workload": "hlu: laplace3d N=%d leaf=256 rank=32 weak admissibility, FP64, 8 rhs, tol 1e-10" % n,
+                      "metric": "time to 1e-10 (getrf + refine)", "value": statistics.median(times), "unit": "s",
+                      "getrf_s": statistics.median(tf), "getrf_device_ms": st["factor_ms"],
+                      "refine_s": statistics.median(times) - statistics.median(tf), "iterations": its,
+                      "residual": res, "residual_recomputed": rel, "launches_per_getrf": st["launches"],
+                      "levels": M.levels, "build_s": t_build, "steps": args.steps, "warmup": args.warmup}),
+          flush=True)
+    M.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile-case", default=None, help="run a small ncu case instead of the benchmark")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batched", "adjoint"],
-                    help="headline (the bench line); batched / adjoint print their own JSON line")
+    ap.add_argument("--workload", default="headline", choices=["headline", "batched", "adjoint", "hlu"],
+                    help="headline (the bench line); batched / adjoint / hlu print their own JSON line")
+    ap.add_argument("--hlu-n", type=int, default=131072, help="hlu workload: matrix order")
     ap.add_argument("--systems", type=int, default=256)
     ap.add_argument("--batch-grid", type=int, default=16,
                     help="batched workload: CTAs per system of the persistent kernels")
@@ -683,6 +727,9 @@ def main():
         return
     if args.workload == "adjoint":
         workload_adjoint(args)
+        return
+    if args.workload == "hlu":
+        workload_hlu(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -117,6 +117,22 @@ SIGNATURES = {
                                                C.c_void_p, C.c_int64, C.c_int, _dp, _vp]),
     "frank_getrf_dense_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int64, C.c_void_p,
                                             _vp]),
+    "frank_hodlr_create": (C.c_int, [C.c_int64, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "frank_hodlr_destroy": (C.c_int, [_vp]),
+    "frank_hodlr_shape": (C.c_int, [_vp, _i64p, _ip, _ip, _ip]),
+    "frank_hodlr_set_lra": (C.c_int, [_vp, C.c_char_p]),
+    "frank_hodlr_set_dense": (C.c_int, [_vp, C.c_int, _dp, C.c_int64]),
+    "frank_hodlr_set_lowrank": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, _dp]),
+    "frank_hodlr_get_dense": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_int64]),
+    "frank_hodlr_get_lowrank": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]),
+    "frank_hodlr_get_pivots": (C.c_int, [_vp, C.c_int, _ip]),
+    "frank_hodlr_build_kernel": (C.c_int, [_vp, C.c_int, _dp, C.c_int, _dp, _vp]),
+    "frank_hodlr_getrf": (C.c_int, [_vp, _vp]),
+    "frank_hodlr_solve_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int, _vp]),
+    "frank_hodlr_matvec_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, _vp]),
+    "frank_hodlr_refine_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int,
+                                            C.c_double, C.c_int, _ip, _dp, _vp]),
+    "frank_hodlr_stats": (C.c_int, [_vp, _i64p, _dp]),
 }
 
 _lib = None

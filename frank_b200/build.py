@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfrank_b200.so")
-SOURCES = ["api.cu", "ops.cu"]
+SOURCES = ["api.cu", "ops.cu", "hodlr.cu"]
+OBJDIR = os.path.join(LIBDIR, "obj")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -33,11 +34,33 @@ def _deps():
     return files
 
 
+def _stale_objects(force: bool = False):
+    """(source, object) pairs whose object is missing or older than the
+    source or any header."""
+    headers = [f for f in _deps() if not f.endswith(".cu")]
+    newest_header = max(os.path.getmtime(f) for f in headers)
+    out = []
+    for src in SOURCES:
+        obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(
+                newest_header, os.path.getmtime(os.path.join(CSRC, src))):
+            out.append((src, obj))
+    return out
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in _deps())
+    if not all(os.path.getmtime(f) <= t for f in _deps()):
+        return False
+    # objects present (a fresh checkout carries only the library): the library
+    # must also be newer than every object and no object may be stale
+    if os.path.isdir(OBJDIR):
+        objs = [os.path.join(OBJDIR, s.replace(".cu", ".o")) for s in SOURCES]
+        if all(os.path.exists(o) for o in objs):
+            return not _stale_objects() and all(os.path.getmtime(o) <= t for o in objs)
+    return True
 
 
 CPP_DIR = os.path.join(HERE, "cpp")
@@ -63,23 +86,35 @@ def build_cpp(force: bool = False) -> str:
     return CPP_LIB
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    os.makedirs(LIBDIR, exist_ok=True)
-    cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "--threads", "2",
-           "-diag-suppress", "177", *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
+def _compile(src: str, obj: str, verbose: bool) -> None:
+    cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-diag-suppress", "177",
+           "-c", os.path.join(CSRC, src), "-o", obj + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    os.replace(LIB + ".tmp", LIB)
+        raise RuntimeError("nvcc failed on %s:\n%s%s" % (src, res.stdout, res.stderr))
+    os.replace(obj + ".tmp", obj)
     if verbose:
         sys.stdout.write(res.stdout + res.stderr)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile each translation unit to an object under lib/obj (again only when
+    it or a header is newer than its object), in parallel, then link."""
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OBJDIR, exist_ok=True)
+    jobs = _stale_objects(force)
+    if jobs:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+            for f in [ex.submit(_compile, src, obj, verbose) for src, obj in jobs]:
+                f.result()
+    objs = [os.path.join(OBJDIR, s.replace(".cu", ".o")) for s in SOURCES]
+    cmd = [_nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", LIB + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
+    os.replace(LIB + ".tmp", LIB)
     return LIB
-
-
-if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
-    print(build_cpp())

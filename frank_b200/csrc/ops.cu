@@ -628,6 +628,50 @@ int64_t svd_scratch(int m, int n) {
   return (int64_t)(mm + k) * k + 2 * (int64_t)k + 2;
 }
 
+// ---------------------------------------------------------------------------
+// Stream-ordered launches for the H-matrix driver (hodlr.cu): the caller owns
+// the scratch (count x ws doubles) and the error slots, nothing is allocated
+// or synchronised, so a whole factorization can be captured into one graph.
+// ---------------------------------------------------------------------------
+
+int64_t qr_ws(int m, int n) { return (int64_t)m * n + std::min(m, n) + 2; }
+
+int64_t lr_add_ws(int m, int n, int ka, int kb) {
+  const int kt = ka + kb, mx = std::max(m, n);
+  return (int64_t)(m + n) * kt + 2 * kt + 5 * (int64_t)kt * kt + kt + (int64_t)mx * kt + svd_scratch(kt, kt) + 2;
+}
+
+void launch_gemm(cudaStream_t s, int m, int n, int k, int count, double alpha, const double* a, int64_t lda,
+                 int64_t sa, bool ta, const double* b, int64_t ldb, int64_t sb, bool tb, double beta, double* c,
+                 int64_t ldc, int64_t sc) {
+  const int64_t tiles = (int64_t)((m + 63) / 64) * ((n + 63) / 64);
+  k_op_gemm<<<dim3((unsigned)tiles, count), OT, 0, s>>>(m, n, k, alpha, Mat{const_cast<double*>(a), lda, sa}, ta,
+                                                       Mat{const_cast<double*>(b), ldb, sb}, tb, beta,
+                                                       Mat{c, ldc, sc});
+}
+
+void launch_qr(cudaStream_t s, int m, int n, int count, const double* a, int64_t lda, int64_t sa, double* q,
+               int64_t ldq, int64_t sq, double* r, int64_t ldr, int64_t sr, double* scratch, int64_t ws) {
+  k_op_qr<<<count, OT, 0, s>>>(m, n, Mat{const_cast<double*>(a), lda, sa}, Mat{q, ldq, sq}, Mat{r, ldr, sr}, scratch,
+                               ws);
+}
+
+void launch_svd(cudaStream_t s, int m, int n, int count, const double* a, int64_t lda, int64_t sa, double* u,
+                int64_t ldu, int64_t su, double* sv, int64_t ss, double* vt, int64_t ldvt, int64_t svt,
+                double* scratch, int64_t ws, int* err) {
+  k_op_svd<<<count, OT, 0, s>>>(m, n, Mat{const_cast<double*>(a), lda, sa}, Mat{u, ldu, su}, Mat{sv, 1, ss},
+                                Mat{vt, ldvt, svt}, scratch, ws, err);
+}
+
+void launch_lr_add(cudaStream_t s, int m, int n, int count, int kmax, int fast, double* ua, int64_t ldua, int64_t sua,
+                   double* sa, int64_t ldsa, int64_t ssa, double* va, int64_t ldva, int64_t sva, int* ka,
+                   const double* ub, int64_t ldub, int64_t sub, const double* sb, int64_t ldsb, int64_t ssb,
+                   const double* vb, int64_t ldvb, int64_t svb, const int* kb, double* scratch, int64_t ws, int* err) {
+  k_op_lr_add<<<count, OT, 0, s>>>(m, n, kmax, fast, 0.0, Mat{ua, ldua, sua}, Mat{sa, ldsa, ssa}, Mat{va, ldva, sva},
+                                   ka, Mat{const_cast<double*>(ub), ldub, sub}, Mat{const_cast<double*>(sb), ldsb, ssb},
+                                   Mat{const_cast<double*>(vb), ldvb, svb}, kb, scratch, ws, err);
+}
+
 }  // namespace ops
 }  // namespace frank
 

@@ -441,6 +441,69 @@ int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra
 int frank_getrf_dense_noalloc(const double* d_a, int64_t lda, int n, double* d_lu, int64_t ldlu,
                               int* d_ipiv, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Multi-level H-matrices: binary cluster tree, weak admissibility, fixed rank.
+ *
+ * The matrix Hierarchical(kernel, params, n, n, rank, nleaf, admis = 0, 2, 2)
+ * (classes/hierarchical.cpp:49-109 with matrix_initializer.cpp:51-58): every
+ * off-diagonal child at every level is LowRank of rank `rank`, every diagonal
+ * child recurses until it is a dense leaf of order `leaf`.  n / leaf must be
+ * a power of two (levels L = log2(n / leaf)).  Block (level l, index c),
+ * l = 1..L, c = 0..2^l - 1, spans the rows of cluster c of level l and the
+ * columns of its sibling c ^ 1; it is U (s x rank), S (rank x rank),
+ * V (rank x s), s = n >> l, all column-major.  Leaf p (0 .. 2^L - 1) is the
+ * dense diagonal block of rows and columns [p leaf, (p + 1) leaf).
+ * ------------------------------------------------------------------------ */
+typedef struct frank_hodlr frank_hodlr;
+
+/* New H-matrix (all blocks zero); 8 <= leaf <= 512, 1 <= rank <= min(64, leaf). */
+int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out);
+int frank_hodlr_destroy(frank_hodlr* h);
+int frank_hodlr_shape(const frank_hodlr* h, int64_t* n, int* leaf, int* rank, int* levels);
+
+/* LowRank += LowRank of the factorization's updates: "fast_rounded_addition"
+ * (the reference's default for fixed rank, addition.cpp:133-189, 191-203)
+ * or "rounded_addition" (addition.cpp:93-127). */
+int frank_hodlr_set_lra(frank_hodlr* h, const char* name);
+
+/* Host blocks of A_H, column-major (leading dimension ld >= leaf for leaves;
+ * U, S, V packed). */
+int frank_hodlr_set_dense(frank_hodlr* h, int leaf, const double* a, int64_t ld);
+int frank_hodlr_set_lowrank(frank_hodlr* h, int level, int index, const double* U, const double* S,
+                            const double* V);
+/* which = 0: A_H; 1: the factor (leaves: packed LU of dgetrf with the
+ * interchanges applied; LowRank: L blocks (odd index) and U blocks (even)). */
+int frank_hodlr_get_dense(const frank_hodlr* h, int which, int leaf, double* a, int64_t ld);
+int frank_hodlr_get_lowrank(const frank_hodlr* h, int which, int level, int index, double* U, double* S,
+                            double* V);
+/* 0-based LAPACK-style pivots of leaf p's getrf. */
+int frank_hodlr_get_pivots(const frank_hodlr* h, int leaf, int* ipiv);
+
+/* Build A_H on the device from points (dim x n, axis-major): dense leaves by
+ * kernel evaluation, every LowRank block by LowRank(Dense, rank)
+ * (low_rank.cpp:40-48 -> rsvd.cpp:17-29, sample min(rank + 5, s), the
+ * reference's Omega: uniform [0,1) from std::mt19937 seeded 0,
+ * functions.cpp:52-66) without storing the block: A Omega and A^T Q are
+ * evaluated tile by tile.  kparams as for frank_blr_build_kernel. */
+int frank_hodlr_build_kernel(frank_hodlr* h, int kernel, const double* points, int dim, const double* kparams,
+                             void* stream);
+
+/* getrf(A) (operations/LAPACK/getrf.cpp:45-65, recursive): the factorization
+ * is captured once into a CUDA graph and replayed from A_H on every call. */
+int frank_hodlr_getrf(frank_hodlr* h, void* stream);
+/* b <- (L U)^{-1} P b in place: trsm(L, b, Lower) then trsm(U, b, Upper)
+ * (examples/h_lu.cpp:45-48); device buffer n x nrhs, ld ldb. */
+int frank_hodlr_solve_device(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, void* stream);
+/* y = A_H x (FP64; gemm(H, x, y) over the leaves and every LowRank block). */
+int frank_hodlr_matvec_device(frank_hodlr* h, const double* d_x, int64_t ldx, double* d_y, int64_t ldy, int nrhs,
+                              void* stream);
+/* x = solve(b), then x += solve(b - A_H x) until every column's
+ * ||b - A_H x|| / ||b|| <= tol (or max_iter corrections). */
+int frank_hodlr_refine_device(frank_hodlr* h, const double* d_b, int64_t ldb, double* d_x, int64_t ldx, int nrhs,
+                              double tol, int max_iter, int* iters, double* relres, void* stream);
+/* Kernel launches of one factorization and the device time of the last getrf (ms). */
+int frank_hodlr_stats(const frank_hodlr* h, int64_t* launches, double* factor_ms);
+
 #ifdef __cplusplus
 }
 #endif
