@@ -34,16 +34,28 @@ def _deps():
     return files
 
 
+def _includes(path: str, seen=None):
+    """The file and every project header it includes (#include "..."), transitively."""
+    import re
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read(), re.M):
+            _includes(os.path.join(os.path.dirname(path), name), seen)
+    return seen
+
+
 def _stale_objects(force: bool = False):
     """(source, object) pairs whose object is missing or older than the
-    source or any header."""
-    headers = [f for f in _deps() if not f.endswith(".cu")]
-    newest_header = max(os.path.getmtime(f) for f in headers)
+    source or a header it includes."""
     out = []
     for src in SOURCES:
         obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
-        if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(
-                newest_header, os.path.getmtime(os.path.join(CSRC, src))):
+        newest = max(os.path.getmtime(f) for f in _includes(os.path.join(CSRC, src)))
+        if force or not os.path.exists(obj) or os.path.getmtime(obj) < newest:
             out.append((src, obj))
     return out
 

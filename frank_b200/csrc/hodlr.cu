@@ -49,6 +49,7 @@ namespace blr = frank_blr_private;
 #undef frank
 
 #include "../../include/frank_b200.h"
+#include "ops_tasks.h"
 
 #include <algorithm>
 #include <cmath>
@@ -71,10 +72,10 @@ void launch_qr(cudaStream_t s, int m, int n, int count, const double* a, int64_t
 void launch_svd(cudaStream_t s, int m, int n, int count, const double* a, int64_t lda, int64_t sa, double* u,
                 int64_t ldu, int64_t su, double* sv, int64_t ss, double* vt, int64_t ldvt, int64_t svt,
                 double* scratch, int64_t ws, int* err);
-void launch_lr_add(cudaStream_t s, int m, int n, int count, int kmax, int fast, double* ua, int64_t ldua, int64_t sua,
-                   double* sa, int64_t ldsa, int64_t ssa, double* va, int64_t ldva, int64_t sva, int* ka,
-                   const double* ub, int64_t ldub, int64_t sub, const double* sb, int64_t ldsb, int64_t ssb,
-                   const double* vb, int64_t ldvb, int64_t svb, const int* kb, double* scratch, int64_t ws, int* err);
+int lr_add_shm_bytes(int ka, int kb);
+int lr_add_prepare(int bytes);
+void launch_lr_add_tasks(cudaStream_t s, int count, const LrAddTask* tasks, int kmax, int fast, double* scratch,
+                         int* err, int shm_bytes);
 }  // namespace ops
 }  // namespace frank
 
@@ -163,6 +164,7 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
 #pragma unroll
       for (int c = 0; c < WCW; ++c) acc[c] = 0.0;
       if (J.mode == 2) {
+#pragma unroll 8
         for (int j = i; j < b; ++j) {
           const double a = Op[i + (int64_t)j * b];
 #pragma unroll
@@ -171,6 +173,7 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
       } else {
         // Linv is unit lower (diagonal not read); Uinv^T is lower with its diagonal
         const int jend = J.mode == 0 ? i : i + 1;
+#pragma unroll 8
         for (int j = 0; j < jend; ++j) {
           const double a = Op[i + (int64_t)j * b];
 #pragma unroll
@@ -436,7 +439,7 @@ __global__ void k_h_omega(int64_t s, int p, int nblk, const double* om, double* 
   }
 }
 
-// After the SVD of Z = K(C, R) Q = U2 diag(sv) Vt2 (Q^T A = Vt2^T diag(sv)
+// After the SVD Z = K(C, R) Q = U2 diag(sv) Vt2 (Q^T A = Vt2^T diag(sv)
 // U2^T): V (k x s, ld k) = U2(:, :k)^T and S = diag(sv(:k)) of every block
 // of a level.
 __global__ void k_h_finish_v(int64_t s, int p, int k, int nblk, const double* U2, const double* sv, double* V,
@@ -607,8 +610,12 @@ struct frank_hodlr {
   double* Sp = nullptr;             // S' of one update (k x k)
   double* core_part = nullptr;      // [CORE_GRID][k*k]
   double* Wu = nullptr;             // U_low S' (n/2 x k)
-  double* lr_scratch = nullptr;     // largest (blocks of a level and parity) x addition scratch
+  double* lr_scratch = nullptr;     // addition scratch of the largest update
   int64_t lr_cap = 0;
+  ::frank::ops::LrAddTask* tasks_d = nullptr;   // every update's additions, in launch order
+  std::vector<::frank::ops::LrAddTask> tasks_h;
+  int64_t ntasks_cap = 0;
+  int lr_shm = 0;
   double* mv_part = nullptr;
   int64_t mv_part_cap = 0;
   double* work = nullptr;           // refinement: residual / correction (n x nrhs)
@@ -715,22 +722,35 @@ void enqueue_update(frank_hodlr* h, int lr, int cr, const double* Ux, const doub
   ::frank::ops::launch_gemm(s, b, b, k, nleaf, 1.0, h->Wu, sn, b, false, Vx, k, (int64_t)b * k, false, 1.0,
                             h->D + (int64_t)pf * b * b, b, (int64_t)b * b);
   h->launches += 2;
-  // LowRank blocks of the node, level by level, even and odd blocks apart
+  // LowRank blocks of the node (every level below it): one addition per block,
+  // all in one launch from the task table
+  const int64_t t0 = (int64_t)h->tasks_h.size();
+  int64_t off = 0;
+  int idx = 0;
   for (int j = lr + 1; j <= h->L; ++j) {
     const int64_t sj = s_of(h, j);
     const int cbase = cr << (j - lr);
-    const int cnt = 1 << (j - lr - 1);
-    for (int par = 0; par < 2; ++par) {
-      const int c0 = cbase + par;
-      const int64_t roff = (int64_t)par * sj;            // rows of block c0 within the node
-      const int64_t coff = (int64_t)(1 - par) * sj;      // columns (cluster c0 ^ 1)
-      ::frank::ops::launch_lr_add(s, (int)sj, (int)sj, cnt, k, h->fast, h->U + u_off(h, j, c0), sj, 2 * sj * k,
-                                  h->S + s_off(h, j, c0), k, 2 * (int64_t)k * k, h->V + u_off(h, j, c0), k,
-                                  2 * sj * k, h->kfill, Ux + roff, sn, 2 * sj, h->Sp, k, 0, Vx + coff * k, k,
-                                  2 * sj * k, h->kfill, h->lr_scratch, ::frank::ops::lr_add_ws((int)sj, (int)sj, k, k),
-                                  h->err + hk::HERR_JACOBI);
-      ++h->launches;
+    for (int c = cbase; c < cbase + (1 << (j - lr)); ++c, ++idx) {
+      ::frank::ops::LrAddTask t;
+      t.ua = h->U + u_off(h, j, c);
+      t.sa = h->S + s_off(h, j, c);
+      t.va = h->V + u_off(h, j, c);
+      t.ub = Ux + (int64_t)(c - cbase) * sj;                    // rows of cluster c within the node
+      t.sb = h->Sp;
+      t.vb = Vx + (int64_t)((c ^ 1) - cbase) * sj * k;          // columns of its sibling
+      t.ldua = sj; t.ldsa = k; t.ldva = k; t.ldub = sn; t.ldsb = k; t.ldvb = k;
+      t.scratch_off = off;
+      t.ka = h->kfill + idx;
+      t.kb = h->kfill + idx;
+      t.m = t.n = (int)sj;
+      h->tasks_h.push_back(t);
+      off += ::frank::ops::lr_add_ws((int)sj, (int)sj, k, k);
     }
+  }
+  if (idx > 0) {
+    ::frank::ops::launch_lr_add_tasks(s, idx, h->tasks_d + t0, k, h->fast, h->lr_scratch, h->err + hk::HERR_JACOBI,
+                                      h->lr_shm);
+    ++h->launches;
   }
 }
 
@@ -766,6 +786,7 @@ int enqueue_factor(frank_hodlr* h, cudaStream_t s) {
   H_TRY(cudaMemcpyAsync(h->S, h->S0, sizeof(double) * (size_t)nblocks_s(h) * h->k * h->k, cudaMemcpyDeviceToDevice, s));
   H_TRY(cudaMemsetAsync(h->err, 0, sizeof(int) * hk::HERR_SLOTS, s));
   h->launches = 0;
+  h->tasks_h.clear();
   enqueue_node(h, 0, 0, s);
   H_TRY(cudaGetLastError());
   return FRANK_OK;
@@ -787,7 +808,7 @@ void free_plan(frank_hodlr* h) {
                   (void*)h->V, (void*)h->Linv, (void*)h->Uinv, (void*)h->UinvT, (void*)h->perm, (void*)h->ipiv,
                   (void*)h->getrf_scratch, (void*)h->geom, (void*)h->flops, (void*)h->err, (void*)h->kfill,
                   (void*)h->counter, (void*)h->Sp, (void*)h->core_part, (void*)h->Wu, (void*)h->lr_scratch,
-                  (void*)h->mv_part, (void*)h->work, (void*)h->nrm})
+                  (void*)h->mv_part, (void*)h->work, (void*)h->nrm, (void*)h->tasks_d})
     if (p) cudaFree(p);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
@@ -887,15 +908,22 @@ int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out) {
   A(dalloc(&h->kfill, P)); A(dalloc(&h->counter, 1));
   A(dalloc(&h->Sp, (size_t)rank * rank)); A(dalloc(&h->core_part, (size_t)CORE_GRID * rank * rank));
   A(dalloc(&h->Wu, (size_t)(n / 2) * rank));
-  // LowRank-addition scratch: the largest batch of one level and parity
-  int64_t cap = 0;
-  for (int lr = 1; lr <= L; ++lr)
-    for (int j = lr + 1; j <= L; ++j) {
-      const int64_t sj = n >> j;
-      cap = std::max(cap, ((int64_t)1 << (j - lr - 1)) * ::frank::ops::lr_add_ws((int)sj, (int)sj, rank, rank));
-    }
+  // LowRank additions: scratch of the largest update (all blocks below a
+  // node at level lr), task table of all updates
+  int64_t cap = 0, ntask = 0;
+  for (int lr = 1; lr <= L; ++lr) {
+    int64_t upd = 0;
+    for (int j = lr + 1; j <= L; ++j)
+      upd += ((int64_t)1 << (j - lr)) * ::frank::ops::lr_add_ws((int)(n >> j), (int)(n >> j), rank, rank);
+    cap = std::max(cap, upd);
+    // one update per node of level lr - 1 (into its right child at level lr)
+    ntask += ((int64_t)1 << (lr - 1)) * (((int64_t)1 << (L - lr + 1)) - 2);
+  }
   if (cap > 0) A(dalloc(&h->lr_scratch, (size_t)cap));
   h->lr_cap = cap;
+  h->ntasks_cap = ntask;
+  A(cudaMalloc(reinterpret_cast<void**>(&h->tasks_d), sizeof(::frank::ops::LrAddTask) * std::max<int64_t>(ntask, 1)));
+  h->lr_shm = ::frank::ops::lr_add_shm_bytes(rank, rank);
   A(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
   A(cudaEventCreate(&h->e0));
   A(cudaEventCreate(&h->e1));
@@ -914,6 +942,7 @@ int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out) {
   A(cudaMemset(h->V0, 0, sizeof(double) * nk));
   A(cudaMemset(h->S0, 0, sizeof(double) * sk));
   A(cudaFuncSetAttribute(blr::k_trinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, blr::TRINV_SMEM_MAX));
+  if (e == cudaSuccess && h->lr_shm > 0 && ::frank::ops::lr_add_prepare(h->lr_shm) != FRANK_OK) h->lr_shm = 0;
   if (e != cudaSuccess) {
     free_plan(h);
     return hfail(FRANK_ERR_CUDA, std::string("H-matrix set-up: ") + cudaGetErrorString(e));
@@ -1033,7 +1062,7 @@ int frank_hodlr_build_kernel(frank_hodlr* h, int kernel, const double* points, i
   // the block is never stored: Y = A Omega and Z = A^T Q evaluate it tile by tile.
   int rc = FRANK_OK;
   double *W = nullptr, *Y = nullptr, *Q = nullptr, *R = nullptr, *Z = nullptr, *U2 = nullptr, *sv = nullptr,
-         *Vt2 = nullptr, *om = nullptr, *sc = nullptr;
+         *Vt2 = nullptr, *Ur = nullptr, *om = nullptr, *sc = nullptr;
   int* errd = h->err;
   const int64_t pmax = std::min<int64_t>(k + 5, h->b);
   const size_t slab = (size_t)n * pmax;   // one level: 2^l blocks of s_l x p
@@ -1043,10 +1072,11 @@ int frank_hodlr_build_kernel(frank_hodlr* h, int kernel, const double* points, i
   for (int l = 1; l <= h->L; ++l) {
     const int64_t sl = s_of(h, l);
     const int p = (int)std::min<int64_t>(k + 5, sl);
-    ws_max = std::max(ws_max, std::max(::frank::ops::qr_ws((int)sl, p), ::frank::ops::svd_scratch((int)sl, p)) << l);
+    ws_max = std::max(ws_max, std::max(::frank::ops::qr_ws((int)sl, p), ::frank::ops::svd_scratch(p, p)) << l);
   }
   A(dalloc(&W, slab)); A(dalloc(&Y, slab)); A(dalloc(&Q, slab)); A(dalloc(&Z, slab)); A(dalloc(&U2, slab));
   A(dalloc(&R, (size_t)pmax * pmax << h->L)); A(dalloc(&Vt2, (size_t)pmax * pmax << h->L));
+  A(dalloc(&Ur, (size_t)pmax * pmax << h->L));
   A(dalloc(&sv, (size_t)pmax << h->L)); A(dalloc(&om, (size_t)(n / 2) * pmax)); A(dalloc(&sc, (size_t)ws_max));
   A(cudaMemsetAsync(errd, 0, sizeof(int) * hk::HERR_SLOTS, s));
   for (int l = 1; l <= h->L && e == cudaSuccess; ++l) {
@@ -1066,19 +1096,25 @@ int frank_hodlr_build_kernel(frank_hodlr* h, int kernel, const double* points, i
     ::frank::ops::launch_qr(s, (int)sl, p, nb, Y, sl, sl * p, Q, sl, sl * p, R, p, (int64_t)p * p, sc,
                             ::frank::ops::qr_ws((int)sl, p));
     hk::k_h_kgemm<<<dim3((unsigned)((sl + 63) / 64), nb), hk::WT, 0, s>>>(K, sl, p, 1, Q, Z);
-    ::frank::ops::launch_svd(s, (int)sl, p, nb, Z, sl, sl * p, U2, sl, sl * p, sv, p, Vt2, p, (int64_t)p * p, sc,
-                             ::frank::ops::svd_scratch((int)sl, p), errd + hk::HERR_JACOBI);
-    // U = Q Vt2(:k, :)^T, V = U2(:, :k)^T, S = diag(sv(:k))
+    // Z = A^T Q = Qz Rz, Rz = Ur diag(sv) Vt2: the SVD of the small Rz only
+    // (Q^T A = Vt2^T diag(sv) (Qz Ur)^T)
+    ::frank::ops::launch_qr(s, (int)sl, p, nb, Z, sl, sl * p, U2, sl, sl * p, R, p, (int64_t)p * p, sc,
+                            ::frank::ops::qr_ws((int)sl, p));
+    ::frank::ops::launch_svd(s, p, p, nb, R, p, (int64_t)p * p, Ur, p, (int64_t)p * p, sv, p, Vt2, p,
+                             (int64_t)p * p, sc, ::frank::ops::svd_scratch(p, p), errd + hk::HERR_JACOBI);
+    ::frank::ops::launch_gemm(s, (int)sl, p, p, nb, 1.0, U2, sl, sl * p, false, Ur, p, (int64_t)p * p, false, 0.0, Z,
+                              sl, sl * p);
+    // U = Q Vt2(:k, :)^T, V = (Qz Ur)(:, :k)^T, S = diag(sv(:k))
     ::frank::ops::launch_gemm(s, (int)sl, k, p, nb, 1.0, Q, sl, sl * p, false, Vt2, p, (int64_t)p * p, true, 0.0,
                               h->U0 + u_off(h, l, 0), sl, sl * k);
-    hk::k_h_finish_v<<<4 * h->sm_count, 256, 0, s>>>(sl, p, k, nb, U2, sv, h->V0 + u_off(h, l, 0),
+    hk::k_h_finish_v<<<4 * h->sm_count, 256, 0, s>>>(sl, p, k, nb, Z, sv, h->V0 + u_off(h, l, 0),
                                                      h->S0 + s_off(h, l, 0));
     A(cudaGetLastError());
     A(cudaStreamSynchronize(s));
   }
   A(cudaStreamSynchronize(s));
-  for (void* ptr : {(void*)W, (void*)Y, (void*)Q, (void*)R, (void*)Z, (void*)U2, (void*)sv, (void*)Vt2, (void*)om,
-                    (void*)sc, (void*)dx})
+  for (void* ptr : {(void*)W, (void*)Y, (void*)Q, (void*)R, (void*)Z, (void*)U2, (void*)sv, (void*)Vt2, (void*)Ur,
+                    (void*)om, (void*)sc, (void*)dx})
     if (ptr) cudaFree(ptr);
   if (e != cudaSuccess) return hfail(FRANK_ERR_CUDA, std::string("H-matrix construction: ") + cudaGetErrorString(e));
   int eh[hk::HERR_SLOTS];
@@ -1107,6 +1143,10 @@ int frank_hodlr_getrf(frank_hodlr* h, void* stream) {
     const cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) return hfail(FRANK_ERR_CUDA, std::string("H-LU graph: ") + cudaGetErrorString(ie));
+    if ((int64_t)h->tasks_h.size() > h->ntasks_cap) return hfail(FRANK_ERR_INVALID, "H-LU: task table overflow");
+    if (!h->tasks_h.empty())
+      H_TRY(cudaMemcpy(h->tasks_d, h->tasks_h.data(), sizeof(::frank::ops::LrAddTask) * h->tasks_h.size(),
+                       cudaMemcpyHostToDevice));
   }
   H_TRY(cudaEventRecord(h->e0, s));
   H_TRY(cudaGraphLaunch(h->gexec, s));

@@ -9,6 +9,7 @@
 // Jacobi, CTA GEMM) working on a per-matrix FP64 scratch slot in global
 // memory, allocated from the stream-ordered pool for the call.
 #include "common.cuh"
+#include "ops_tasks.h"
 #include "../../include/frank_b200.h"
 
 #include <algorithm>
@@ -85,13 +86,16 @@ FRANK_D void load_svd(int m, int n, const double* a, int64_t lda, bool trans, do
 // SVD of a (m x n, lda): U (m x k, ldu), s (k), Vt (k x n, ldvt), k = min(m, n),
 // singular values descending; columns with a zero singular value get a zero
 // left vector.  Scratch: (m + n) * k + 2 k doubles.  Returns false on a
-// Jacobi sweep limit.
+// Jacobi sweep limit.  When shm holds at least (max(m, n) + k) k doubles the
+// rotated matrix lives there instead of in the scratch (the sweeps are a
+// chain of dependent column loads, so shared memory's latency sets their
+// pace; the scratch layout is unchanged).
 FRANK_D bool cta_svd(int m, int n, const double* a, int64_t lda, double* U, int64_t ldu, double* s, double* Vt,
-                     int64_t ldvt, double* scratch, int* flag) {
+                     int64_t ldvt, double* scratch, int* flag, double* shm = nullptr, int64_t shm_cap = 0) {
   const bool trans = m < n;
   const int mm = trans ? n : m, k = trans ? m : n;
-  double* G = scratch;
-  double* sig = G + (int64_t)(mm + k) * k;
+  double* G = (shm && (int64_t)(mm + k) * k <= shm_cap) ? shm : scratch;
+  double* sig = scratch + (int64_t)(mm + k) * k;
   int* ord = reinterpret_cast<int*>(sig + k);
   load_svd(m, n, a, lda, trans, G);
   const bool ok = jacobi_svd(mm, k, G, sig, ord, flag);
@@ -353,16 +357,15 @@ __global__ void __launch_bounds__(OT) k_op_rid(int m, int n, int s, int k, Mat A
 // else ka.  fast (fixed rank, Ua and Va^T orthonormal): the projections
 // Zu = Ua^T Ub, Zv = Va Vb^T, QR of the remainders only, core
 // [I Zu; 0 Ru] blockdiag(Sa, Sb) [I Zv; 0 Rv]^T.
-__global__ void __launch_bounds__(OT) k_op_lr_add(int m, int n, int kmax, int fast, double eps, Mat Ua, Mat Sa, Mat Va,
-                                                  int* ka_io, Mat Ub, Mat Sb, Mat Vb, const int* kb_in,
-                                                  double* scratch, int64_t ws, int* err) {
+FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* ua_out, int64_t ldua, double* sa_out,
+                         int64_t ldsa, double* va_out, int64_t ldva, int* ka_io, const double* ub, int64_t ldub,
+                         const double* sb, int64_t ldsb, const double* vb, int64_t ldvb, int kb, double* X, int* err,
+                         double* shm, int64_t shm_cap) {
   __shared__ double gsm[GSM];
   __shared__ double red[32];
   __shared__ int flag, s_rank;
-  const int b = blockIdx.x;
-  const int ka = ka_io[b], kb = kb_in[b];
+  const int ka = *ka_io;
   const int kt = ka + kb;
-  double* X = scratch + (int64_t)b * ws;        // m x kt stacked U side
   double* Y = X + (int64_t)m * kt;              // n x kt stacked V side (V^T columns)
   double* tu = Y + (int64_t)n * kt;             // kt
   double* tv = tu + kt;                         // kt
@@ -374,7 +377,8 @@ __global__ void __launch_bounds__(OT) k_op_lr_add(int m, int n, int kmax, int fa
   double* Vmt = sv + kt;                        // kt x kt
   double* T = Vmt + (int64_t)kt * kt;           // max(m, n) x kt
   double* sc = T + (int64_t)max(m, n) * kt;     // svd scratch (2 kt + 2) kt
-  const double *ua = Ua.at(b), *sa = Sa.at(b), *va = Va.at(b), *ub = Ub.at(b), *sb = Sb.at(b), *vb = Vb.at(b);
+  const double *ua = ua_out, *sa = sa_out, *va = va_out;
+  struct LD { int64_t ld; } Ua{ldua}, Sa{ldsa}, Va{ldva}, Ub{ldub}, Sb{ldsb}, Vb{ldvb};
   const bool use_fast = fast && eps == 0.0 && kt <= m && kt <= n;
   int mu, mv;
   if (!use_fast) {
@@ -440,7 +444,7 @@ __global__ void __launch_bounds__(OT) k_op_lr_add(int m, int n, int kmax, int fa
                          T + (int64_t)ka * kt, kt, gsm);
     cta_gemm<double, OT>(kt, kt, kt, 1.0, T, kt, false, Rv, kt, true, 0.0, M, kt, gsm);
   }
-  if (!cta_svd(mu, mv, M, mu, Um, mu, sv, Vmt, min(mu, mv), sc, &flag) && threadIdx.x == 0)
+  if (!cta_svd(mu, mv, M, mu, Um, mu, sv, Vmt, min(mu, mv), sc, &flag, shm, shm_cap) && threadIdx.x == 0)
     atomicAdd(err + OPS_ERR_JACOBI, 1);
   const int nsv = min(mu, mv);
   if (threadIdx.x == 0) {
@@ -467,8 +471,6 @@ __global__ void __launch_bounds__(OT) k_op_lr_add(int m, int n, int kmax, int fa
   const int r = s_rank;
   const int ldvm = nsv;
   // U = [Q_u-side] Um(:, :r): rounded: Qu [Um; 0]; fast: [Ua | Qu] Um
-  double* ua_out = Ua.at(b);
-  double* va_out = Va.at(b);
   for (int side = 0; side < 2; ++side) {
     const int rows = side ? n : m;
     double* St = side ? Y : X;
@@ -507,12 +509,31 @@ __global__ void __launch_bounds__(OT) k_op_lr_add(int m, int n, int kmax, int fa
     }
     __syncthreads();
   }
-  double* sp = Sa.at(b);
+  double* sp = sa_out;
   for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
     const int i = e % r, c = e / r;
     sp[i + (int64_t)c * Sa.ld] = i == c ? sv[i] : 0.0;
   }
-  if (threadIdx.x == 0) ka_io[b] = r;
+  if (threadIdx.x == 0) *ka_io = r;
+}
+
+__global__ void __launch_bounds__(OT) k_op_lr_add(int m, int n, int kmax, int fast, double eps, Mat Ua, Mat Sa, Mat Va,
+                                                  int* ka_io, Mat Ub, Mat Sb, Mat Vb, const int* kb_in,
+                                                  double* scratch, int64_t ws, int* err, int64_t shm_cap) {
+  extern __shared__ double dyn[];
+  const int b = blockIdx.x;
+  lr_add_body(m, n, kmax, fast, eps, Ua.at(b), Ua.ld, Sa.at(b), Sa.ld, Va.at(b), Va.ld, ka_io + b, Ub.at(b), Ub.ld,
+              Sb.at(b), Sb.ld, Vb.at(b), Vb.ld, kb_in[b], scratch + (int64_t)b * ws, err, dyn, shm_cap);
+}
+
+// One LowRank addition per CTA from a task table (blocks of different sizes
+// in one launch).
+__global__ void __launch_bounds__(OT) k_op_lr_add_tasks(const LrAddTask* tasks, int kmax, int fast, double* scratch,
+                                                        int* err, int64_t shm_cap) {
+  extern __shared__ double dyn[];
+  const LrAddTask t = tasks[blockIdx.x];
+  lr_add_body(t.m, t.n, kmax, fast, 0.0, t.ua, t.ldua, t.sa, t.ldsa, t.va, t.ldva, t.ka, t.ub, t.ldub, t.sb, t.ldsb,
+              t.vb, t.ldvb, *t.kb, scratch + t.scratch_off, err, dyn, shm_cap);
 }
 
 // C = alpha op(A) op(B) + beta C (operations/BLAS/gemm.cpp:126-146,
@@ -663,13 +684,25 @@ void launch_svd(cudaStream_t s, int m, int n, int count, const double* a, int64_
                                 Mat{vt, ldvt, svt}, scratch, ws, err);
 }
 
-void launch_lr_add(cudaStream_t s, int m, int n, int count, int kmax, int fast, double* ua, int64_t ldua, int64_t sua,
-                   double* sa, int64_t ldsa, int64_t ssa, double* va, int64_t ldva, int64_t sva, int* ka,
-                   const double* ub, int64_t ldub, int64_t sub, const double* sb, int64_t ldsb, int64_t ssb,
-                   const double* vb, int64_t ldvb, int64_t svb, const int* kb, double* scratch, int64_t ws, int* err) {
-  k_op_lr_add<<<count, OT, 0, s>>>(m, n, kmax, fast, 0.0, Mat{ua, ldua, sua}, Mat{sa, ldsa, ssa}, Mat{va, ldva, sva},
-                                   ka, Mat{const_cast<double*>(ub), ldub, sub}, Mat{const_cast<double*>(sb), ldsb, ssb},
-                                   Mat{const_cast<double*>(vb), ldvb, svb}, kb, scratch, ws, err);
+// Shared memory (bytes) for the core SVD of an addition of ranks ka + kb,
+// or 0 when it does not fit beside the kernel's static arrays.
+int lr_add_shm_bytes(int ka, int kb) {
+  const int64_t kt = ka + kb, b = (2 * kt) * kt * (int64_t)sizeof(double);
+  return b <= 160 * 1024 ? (int)b : 0;
+}
+
+// Opt the addition kernels in to the shared memory of lr_add_shm_bytes (once,
+// outside any stream capture).
+int lr_add_prepare(int bytes) {
+  if (cudaFuncSetAttribute(k_op_lr_add, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(k_op_lr_add_tasks, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+    return set_error(FRANK_ERR_CUDA, "LowRank addition: shared memory attribute");
+  return FRANK_OK;
+}
+
+void launch_lr_add_tasks(cudaStream_t s, int count, const LrAddTask* tasks, int kmax, int fast, double* scratch,
+                         int* err, int shm_bytes) {
+  k_op_lr_add_tasks<<<count, OT, shm_bytes, s>>>(tasks, kmax, fast, scratch, err, shm_bytes / (int)sizeof(double));
 }
 
 }  // namespace ops
@@ -901,7 +934,7 @@ int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra
     k_op_lr_add<<<count, OT, 0, s>>>(m, n, kmax, fast, eps, Mat{d_ua, ldua, sua}, Mat{d_sa, ldsa, ssa},
                                      Mat{d_va, ldva, sva}, d_ka, Mat{const_cast<double*>(d_ub), ldub, sub},
                                      Mat{const_cast<double*>(d_sb), ldsb, ssb},
-                                     Mat{const_cast<double*>(d_vb), ldvb, svb}, d_kb, sc, ws, err);
+                                     Mat{const_cast<double*>(d_vb), ldvb, svb}, d_kb, sc, ws, err, 0);
   });
 }
 
