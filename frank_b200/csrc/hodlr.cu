@@ -87,8 +87,11 @@ using blr::kernel_eval;
 
 constexpr int HMAX_RANK = 64;   // k <= 64: two rank rows per lane in the walks
 constexpr int HMAX_LEAF = 512;  // b <= 512
-constexpr int WT = 256;         // threads of the walk / update kernels
+constexpr int WT = 256;         // threads of the update / matvec kernels
+constexpr int WWT = 1024;       // threads of a substitution walk (many loads in flight per SM)
 constexpr int WCW = 4;          // right-hand-side columns per walking CTA
+// dynamic shared memory of a walk: r, per-warp partials, t1, t2
+constexpr int WALK_SMEM = (WCW * HMAX_LEAF + (WWT / 32) * WCW * HMAX_RANK + 2 * WCW * HMAX_RANK) * 8;
 constexpr int KG_P = 72;        // rsvd sample width the construction product holds (k + 5 <= 69)
 
 enum { HERR_JACOBI = 8, HERR_RANK = 9, HERR_SLOTS = 16 };
@@ -133,10 +136,12 @@ struct Walk {
 };
 
 FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
-  __shared__ double r[WCW][HMAX_LEAF];
-  __shared__ double part[WT / 32][WCW][HMAX_RANK];
-  __shared__ double t1[WCW][HMAX_RANK];
-  __shared__ double t2[WCW][HMAX_RANK];
+  extern __shared__ double wsm[];
+  double(*r)[HMAX_LEAF] = reinterpret_cast<double(*)[HMAX_LEAF]>(wsm);
+  double(*part)[WCW][HMAX_RANK] = reinterpret_cast<double(*)[WCW][HMAX_RANK]>(wsm + WCW * HMAX_LEAF);
+  double(*t1)[HMAX_RANK] =
+      reinterpret_cast<double(*)[HMAX_RANK]>(wsm + WCW * HMAX_LEAF + (WWT / 32) * WCW * HMAX_RANK);
+  double(*t2)[HMAX_RANK] = t1 + WCW;
   const int col0 = blockIdx.x * WCW;
   if (col0 >= J.ncols) return;
   const int nc = min(WCW, J.ncols - col0);
@@ -152,14 +157,14 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
     const int64_t pr = (int64_t)p * b - row0;
     // leaf solve
     const int* perm = f.perm + (int64_t)p * b;
-    for (int e = tid; e < WCW * b; e += WT) {
+    for (int e = tid; e < WCW * b; e += WWT) {
       const int c = e / b, i = e % b;
       const int src = J.mode == 0 ? perm[i] : i;
       r[c][i] = c < nc ? B[(pr + src) * rs + c * cs] : 0.0;
     }
     __syncthreads();
     const double* Op = (J.mode == 0 ? f.Linv : (J.mode == 1 ? f.UinvT : f.Uinv)) + (int64_t)p * b * b;
-    for (int i = tid; i < b; i += WT) {
+    for (int i = tid; i < b; i += WWT) {
       double acc[WCW];
 #pragma unroll
       for (int c = 0; c < WCW; ++c) acc[c] = 0.0;
@@ -207,7 +212,7 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
         for (int q = 0; q < 2; ++q)
 #pragma unroll
           for (int c = 0; c < WCW; ++c) acc[q][c] = 0.0;
-        for (int64_t i = wid; i < sl; i += WT / 32) {
+        for (int64_t i = wid; i < sl; i += WWT / 32) {
           double xv[WCW];
 #pragma unroll
           for (int c = 0; c < WCW; ++c) xv[c] = c < nc ? B[(src + i) * rs + c * cs] : 0.0;
@@ -229,7 +234,7 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
             for (int c = 0; c < WCW; ++c) part[wid][c][rr] = acc[q][c];
         }
       } else {
-        for (int rr = wid; rr < k; rr += WT / 32) {
+        for (int rr = wid; rr < k; rr += WWT / 32) {
           double acc[WCW];
 #pragma unroll
           for (int c = 0; c < WCW; ++c) acc[c] = 0.0;
@@ -243,21 +248,21 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
             const double v = blr::warp_sum(acc[c]);
             if (lane == 0) {
               part[0][c][rr] = v;
-              for (int w = 1; w < WT / 32; ++w) part[w][c][rr] = 0.0;
+              for (int w = 1; w < WWT / 32; ++w) part[w][c][rr] = 0.0;
             }
           }
         }
       }
       __syncthreads();
-      for (int e = tid; e < WCW * k; e += WT) {
+      for (int e = tid; e < WCW * k; e += WWT) {
         const int c = e / k, rr = e % k;
         double v = 0.0;
-        for (int w = 0; w < WT / 32; ++w) v += part[w][c][rr];
+        for (int w = 0; w < WWT / 32; ++w) v += part[w][c][rr];
         t1[c][rr] = v;
       }
       __syncthreads();
       // t2 = S t1 (modes 0, 2) or S^T t1 (mode 1)
-      for (int e = tid; e < WCW * k; e += WT) {
+      for (int e = tid; e < WCW * k; e += WWT) {
         const int c = e / k, rr = e % k;
         double v = 0.0;
         for (int q = 0; q < k; ++q) v += (J.mode == 1 ? Sb[q + (int64_t)rr * k] : Sb[rr + (int64_t)q * k]) * t1[c][q];
@@ -265,7 +270,7 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
       }
       __syncthreads();
       // B_dst -= U t2 (modes 0, 2) or V^T t2 (mode 1)
-      for (int64_t i = tid; i < sl; i += WT) {
+      for (int64_t i = tid; i < sl; i += WWT) {
         double acc[WCW];
 #pragma unroll
         for (int c = 0; c < WCW; ++c) acc[c] = 0.0;
@@ -281,7 +286,7 @@ FRANK_D void walk_body(const HView& h, const LeafFactors& f, const Walk& J) {
   }
 }
 
-__global__ void __launch_bounds__(WT) k_h_walk(HView h, LeafFactors f, Walk j0, Walk j1) {
+__global__ void __launch_bounds__(WWT) k_h_walk(HView h, LeafFactors f, Walk j0, Walk j1) {
   walk_body(h, f, blockIdx.y == 0 ? j0 : j1);
 }
 
@@ -605,13 +610,17 @@ struct frank_hodlr {
   int* geom = nullptr;              // leaf BlrView geometry: off {0, b}, dslot {0}, lslot {-1}
   unsigned long long* flops = nullptr;
   int* err = nullptr;
-  int* kfill = nullptr;             // [P] ranks, all k
+  int* kfill = nullptr;             // [L + 1][P] ranks, all k (one row per level's stream)
   int* counter = nullptr;
-  double* Sp = nullptr;             // S' of one update (k x k)
+  double* Sp = nullptr;             // S' of every internal node's update ([2^L - 1][k x k])
   double* core_part = nullptr;      // [CORE_GRID][k*k]
   double* Wu = nullptr;             // U_low S' (n/2 x k)
-  double* lr_scratch = nullptr;     // addition scratch of the largest update
+  double* lr_scratch = nullptr;     // addition scratch, one region per level
   int64_t lr_cap = 0;
+  std::vector<int64_t> lr_base;     // [L + 1] start of level j's region
+  std::vector<cudaStream_t> ls;     // [L + 1] one stream per level for the LowRank additions
+  std::vector<cudaEvent_t> lev;     // [L + 1] last addition enqueued on level j's stream
+  cudaEvent_t ev_fork = nullptr, ev_core = nullptr;
   ::frank::ops::LrAddTask* tasks_d = nullptr;   // every update's additions, in launch order
   std::vector<::frank::ops::LrAddTask> tasks_h;
   int64_t ntasks_cap = 0;
@@ -709,47 +718,52 @@ void enqueue_leaf(frank_hodlr* h, int p, cudaStream_t s) {
   h->launches += 3;
 }
 
-// LowRank(U_x, S', V_x) (n_node x n_node, U_x ld s(lr), V_x ld k) added into
-// node (lr, cr) of the working copy.
-void enqueue_update(frank_hodlr* h, int lr, int cr, const double* Ux, const double* Vx, cudaStream_t s) {
+// LowRank(U_x, S'_node, V_x) (n_node x n_node, U_x ld s(lr), V_x ld k) added
+// into node (lr, cr) of the working copy: the dense leaves on stream s, the
+// LowRank blocks of each level j on that level's stream (after the node's
+// core, event ev_core), so that the additions into blocks needed late (the
+// large ones near the top of the node) run beside the factorization of the
+// node's first children.
+void enqueue_update(frank_hodlr* h, int lr, int cr, const double* Ux, const double* Vx, const double* Sp,
+                    cudaStream_t s) {
   const int k = h->k, b = h->b;
   const int64_t sn = s_of(h, lr);
   // Wu = U_x S'
-  ::frank::ops::launch_gemm(s, (int)sn, k, k, 1, 1.0, Ux, sn, 0, false, h->Sp, k, 0, false, 0.0, h->Wu, sn, 0);
+  ::frank::ops::launch_gemm(s, (int)sn, k, k, 1, 1.0, Ux, sn, 0, false, Sp, k, 0, false, 0.0, h->Wu, sn, 0);
   // dense leaves of the node: D_p += Wu(rows of p) V_x(:, cols of p)
   const int nleaf = 1 << (h->L - lr);
   const int pf = cr << (h->L - lr);
   ::frank::ops::launch_gemm(s, b, b, k, nleaf, 1.0, h->Wu, sn, b, false, Vx, k, (int64_t)b * k, false, 1.0,
                             h->D + (int64_t)pf * b * b, b, (int64_t)b * b);
   h->launches += 2;
-  // LowRank blocks of the node (every level below it): one addition per block,
-  // all in one launch from the task table
-  const int64_t t0 = (int64_t)h->tasks_h.size();
-  int64_t off = 0;
-  int idx = 0;
+  // LowRank blocks of the node, one launch per level from the task table
   for (int j = lr + 1; j <= h->L; ++j) {
     const int64_t sj = s_of(h, j);
     const int cbase = cr << (j - lr);
+    const int64_t t0 = (int64_t)h->tasks_h.size();
+    int64_t off = 0;
+    int idx = 0;
     for (int c = cbase; c < cbase + (1 << (j - lr)); ++c, ++idx) {
       ::frank::ops::LrAddTask t;
       t.ua = h->U + u_off(h, j, c);
       t.sa = h->S + s_off(h, j, c);
       t.va = h->V + u_off(h, j, c);
       t.ub = Ux + (int64_t)(c - cbase) * sj;                    // rows of cluster c within the node
-      t.sb = h->Sp;
+      t.sb = Sp;
       t.vb = Vx + (int64_t)((c ^ 1) - cbase) * sj * k;          // columns of its sibling
       t.ldua = sj; t.ldsa = k; t.ldva = k; t.ldub = sn; t.ldsb = k; t.ldvb = k;
-      t.scratch_off = off;
-      t.ka = h->kfill + idx;
-      t.kb = h->kfill + idx;
+      t.scratch_off = h->lr_base[j] + off;
+      t.ka = h->kfill + (int64_t)j * h->P + idx;
+      t.kb = t.ka;
       t.m = t.n = (int)sj;
       h->tasks_h.push_back(t);
       off += ::frank::ops::lr_add_ws((int)sj, (int)sj, k, k);
     }
-  }
-  if (idx > 0) {
-    ::frank::ops::launch_lr_add_tasks(s, idx, h->tasks_d + t0, k, h->fast, h->lr_scratch, h->err + hk::HERR_JACOBI,
-                                      h->lr_shm);
+    cudaStream_t sj_stream = h->ls[j];
+    cudaStreamWaitEvent(sj_stream, h->ev_core, 0);
+    ::frank::ops::launch_lr_add_tasks(sj_stream, idx, h->tasks_d + t0, k, h->fast, h->lr_scratch,
+                                      h->err + hk::HERR_JACOBI, h->lr_shm);
+    cudaEventRecord(h->lev[j], sj_stream);
     ++h->launches;
   }
 }
@@ -763,18 +777,23 @@ void enqueue_node(frank_hodlr* h, int l, int c, cudaStream_t s) {
   enqueue_node(h, l + 1, 2 * c, s);
   const int up = 2 * c, lo = 2 * c + 1;
   const int64_t sc = s_of(h, l + 1);
+  // the node's own off-diagonal blocks: every addition into them enqueued so far
+  cudaStreamWaitEvent(s, h->lev[l + 1], 0);
   // U_up <- L_left^{-1} P U_up (trsm.cpp:106-115 -> 117-125 -> leaves);
   // V_low <- V_low U_left^{-1}
   hk::Walk j0{0, l + 1, 2 * c, k, h->U + u_off(h, l + 1, up), 1, sc};
   hk::Walk j1{1, l + 1, 2 * c, k, h->V + u_off(h, l + 1, lo), k, 1};
-  hk::k_h_walk<<<dim3((k + hk::WCW - 1) / hk::WCW, 2), hk::WT, 0, s>>>(view(h, true), leaf_factors(h), j0, j1);
-  // S' = -(S_low V_low)(U_up S_up)
+  hk::k_h_walk<<<dim3((k + hk::WCW - 1) / hk::WCW, 2), hk::WWT, hk::WALK_SMEM, s>>>(view(h, true), leaf_factors(h),
+                                                                                   j0, j1);
+  // S' = -(S_low V_low)(U_up S_up), one k x k slot per internal node
+  double* Sp = h->Sp + ((int64_t)(1 << l) - 1 + c) * k * k;
   const int grid = (int)std::min<int64_t>(CORE_GRID, (sc + 511) / 512);
   hk::k_h_core<<<grid, hk::WT, 0, s>>>(sc, k, h->V + u_off(h, l + 1, lo), h->U + u_off(h, l + 1, up),
-                                       h->S + s_off(h, l + 1, lo), h->S + s_off(h, l + 1, up), h->core_part, h->Sp,
+                                       h->S + s_off(h, l + 1, lo), h->S + s_off(h, l + 1, up), h->core_part, Sp,
                                        h->counter);
+  cudaEventRecord(h->ev_core, s);
   h->launches += 2;
-  enqueue_update(h, l + 1, lo, h->U + u_off(h, l + 1, lo), h->V + u_off(h, l + 1, up), s);
+  enqueue_update(h, l + 1, lo, h->U + u_off(h, l + 1, lo), h->V + u_off(h, l + 1, up), Sp, s);
   enqueue_node(h, l + 1, 2 * c + 1, s);
 }
 
@@ -787,7 +806,16 @@ int enqueue_factor(frank_hodlr* h, cudaStream_t s) {
   H_TRY(cudaMemsetAsync(h->err, 0, sizeof(int) * hk::HERR_SLOTS, s));
   h->launches = 0;
   h->tasks_h.clear();
+  H_TRY(cudaEventRecord(h->ev_fork, s));
+  for (int j = 1; j <= h->L; ++j) {
+    H_TRY(cudaStreamWaitEvent(h->ls[j], h->ev_fork, 0));
+    H_TRY(cudaEventRecord(h->lev[j], h->ls[j]));
+  }
   enqueue_node(h, 0, 0, s);
+  for (int j = 1; j <= h->L; ++j) {
+    H_TRY(cudaEventRecord(h->lev[j], h->ls[j]));
+    H_TRY(cudaStreamWaitEvent(s, h->lev[j], 0));
+  }
   H_TRY(cudaGetLastError());
   return FRANK_OK;
 }
@@ -812,6 +840,10 @@ void free_plan(frank_hodlr* h) {
     if (p) cudaFree(p);
   if (h->e0) cudaEventDestroy(h->e0);
   if (h->e1) cudaEventDestroy(h->e1);
+  for (cudaStream_t x : h->ls) if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t x : h->lev) if (x) cudaEventDestroy(x);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_core) cudaEventDestroy(h->ev_core);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
 }
@@ -863,9 +895,9 @@ int enqueue_solve(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, cudaStream
   const hk::LeafFactors f = leaf_factors(h);
   const unsigned g = (unsigned)((nrhs + hk::WCW - 1) / hk::WCW);
   hk::Walk fw{0, 0, 0, nrhs, d_b, 1, ldb}, none{0, 0, 0, 0, nullptr, 1, 1};
-  hk::k_h_walk<<<dim3(g, 1), hk::WT, 0, s>>>(v, f, fw, none);
+  hk::k_h_walk<<<dim3(g, 1), hk::WWT, hk::WALK_SMEM, s>>>(v, f, fw, none);
   hk::Walk bw{2, 0, 0, nrhs, d_b, 1, ldb};
-  hk::k_h_walk<<<dim3(g, 1), hk::WT, 0, s>>>(v, f, bw, none);
+  hk::k_h_walk<<<dim3(g, 1), hk::WWT, hk::WALK_SMEM, s>>>(v, f, bw, none);
   H_TRY(cudaGetLastError());
   return FRANK_OK;
 }
@@ -905,24 +937,31 @@ int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out) {
   A(dalloc(&h->perm, P * leaf)); A(dalloc(&h->ipiv, P * leaf));
   A(dalloc(&h->getrf_scratch, (size_t)leaf * leaf + 32 * leaf));
   A(dalloc(&h->geom, 4)); A(dalloc(&h->flops, blr::FLOP_SLOTS)); A(dalloc(&h->err, hk::HERR_SLOTS));
-  A(dalloc(&h->kfill, P)); A(dalloc(&h->counter, 1));
-  A(dalloc(&h->Sp, (size_t)rank * rank)); A(dalloc(&h->core_part, (size_t)CORE_GRID * rank * rank));
+  A(dalloc(&h->kfill, (size_t)(L + 1) * P)); A(dalloc(&h->counter, 1));
+  A(dalloc(&h->Sp, (size_t)P * rank * rank)); A(dalloc(&h->core_part, (size_t)CORE_GRID * rank * rank));
   A(dalloc(&h->Wu, (size_t)(n / 2) * rank));
-  // LowRank additions: scratch of the largest update (all blocks below a
-  // node at level lr), task table of all updates
+  // LowRank additions: per level j a scratch region for its largest launch
+  // (2^(j-1) blocks of order n >> j, the update of the root's right child),
+  // and the task table of all updates
   int64_t cap = 0, ntask = 0;
-  for (int lr = 1; lr <= L; ++lr) {
-    int64_t upd = 0;
-    for (int j = lr + 1; j <= L; ++j)
-      upd += ((int64_t)1 << (j - lr)) * ::frank::ops::lr_add_ws((int)(n >> j), (int)(n >> j), rank, rank);
-    cap = std::max(cap, upd);
-    // one update per node of level lr - 1 (into its right child at level lr)
-    ntask += ((int64_t)1 << (lr - 1)) * (((int64_t)1 << (L - lr + 1)) - 2);
+  h->lr_base.assign(L + 2, 0);
+  for (int j = 1; j <= L; ++j) {
+    h->lr_base[j] = cap;
+    if (j >= 2) cap += ((int64_t)1 << (j - 1)) * ::frank::ops::lr_add_ws((int)(n >> j), (int)(n >> j), rank, rank);
   }
+  for (int lr = 1; lr <= L; ++lr) ntask += ((int64_t)1 << (lr - 1)) * (((int64_t)1 << (L - lr + 1)) - 2);
   if (cap > 0) A(dalloc(&h->lr_scratch, (size_t)cap));
   h->lr_cap = cap;
   h->ntasks_cap = ntask;
   A(cudaMalloc(reinterpret_cast<void**>(&h->tasks_d), sizeof(::frank::ops::LrAddTask) * std::max<int64_t>(ntask, 1)));
+  h->ls.assign(L + 1, nullptr);
+  h->lev.assign(L + 1, nullptr);
+  for (int j = 0; j <= L; ++j) {
+    A(cudaStreamCreateWithFlags(&h->ls[j], cudaStreamNonBlocking));
+    A(cudaEventCreateWithFlags(&h->lev[j], cudaEventDisableTiming));
+  }
+  A(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&h->ev_core, cudaEventDisableTiming));
   h->lr_shm = ::frank::ops::lr_add_shm_bytes(rank, rank);
   A(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
   A(cudaEventCreate(&h->e0));
@@ -932,7 +971,7 @@ int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out) {
     return hfail(FRANK_ERR_CUDA, std::string("H-matrix allocation: ") + cudaGetErrorString(e));
   }
   const int geom[4] = {0, leaf, 0, -1};
-  std::vector<int> kf((size_t)P, rank);
+  std::vector<int> kf((size_t)(L + 1) * P, rank);
   A(cudaMemcpy(h->geom, geom, sizeof(geom), cudaMemcpyHostToDevice));
   A(cudaMemcpy(h->kfill, kf.data(), sizeof(int) * kf.size(), cudaMemcpyHostToDevice));
   A(cudaMemset(h->counter, 0, sizeof(int)));
@@ -942,6 +981,7 @@ int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out) {
   A(cudaMemset(h->V0, 0, sizeof(double) * nk));
   A(cudaMemset(h->S0, 0, sizeof(double) * sk));
   A(cudaFuncSetAttribute(blr::k_trinv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, blr::TRINV_SMEM_MAX));
+  A(cudaFuncSetAttribute(hk::k_h_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, hk::WALK_SMEM));
   if (e == cudaSuccess && h->lr_shm > 0 && ::frank::ops::lr_add_prepare(h->lr_shm) != FRANK_OK) h->lr_shm = 0;
   if (e != cudaSuccess) {
     free_plan(h);
