@@ -463,6 +463,114 @@ __global__ void k_h_finish_v(int64_t s, int p, int k, int nblk, const double* U2
   }
 }
 
+constexpr int MV_CHUNK = 1024;
+
+// Level-parallel solve.  With W_X = M_right(U_low) and Z_X = U_left^{-1} U_up
+// precomputed per node X (M = the permuted forward substitution of a
+// subtree), L^{-1} P b and U^{-1} y are: every leaf at once, then for each
+// level from the bottom up, every node at once: x_right -= W_X S_low V_low
+// x_left (forward), x_left -= Z_X S_up V_up x_right (backward).
+//
+// Leaves: x_p <- Linv_p P_p x_p (mode 0) or Uinv_p x_p (mode 2); grid: leaves x
+// column groups of WCW.
+__global__ void __launch_bounds__(WT) k_h_leaf_apply(int b, int mode, LeafFactors f, double* x, int64_t ldx,
+                                                     int nrhs) {
+  __shared__ double r[WCW][HMAX_LEAF];
+  const int p = blockIdx.x, c0 = blockIdx.y * WCW;
+  const int nc = min(WCW, nrhs - c0);
+  const int* perm = f.perm + (int64_t)p * b;
+  double* xp = x + (int64_t)p * b + (int64_t)c0 * ldx;
+  for (int e = threadIdx.x; e < WCW * b; e += WT) {
+    const int c = e / b, i = e % b;
+    r[c][i] = c < nc ? xp[(mode == 0 ? perm[i] : i) + c * ldx] : 0.0;
+  }
+  __syncthreads();
+  const double* Op = (mode == 0 ? f.Linv : f.Uinv) + (int64_t)p * b * b;
+  for (int i = threadIdx.x; i < b; i += WT) {
+    double acc[WCW];
+#pragma unroll
+    for (int c = 0; c < WCW; ++c) acc[c] = mode == 0 ? r[c][i] : 0.0;
+    const int j0 = mode == 0 ? 0 : i, j1 = mode == 0 ? i : b;
+#pragma unroll 8
+    for (int j = j0; j < j1; ++j) {
+      const double a = Op[i + (int64_t)j * b];
+#pragma unroll
+      for (int c = 0; c < WCW; ++c) acc[c] += a * r[c][j];
+    }
+    for (int c = 0; c < nc; ++c) xp[i + c * ldx] = acc[c];
+  }
+}
+
+// Partials T[node][chunk] (k x nrhs) = V_c(:, chunk) x(cols of c, chunk) for
+// the blocks c = 2 node + parity of level l (grid: chunks x nodes).
+__global__ void __launch_bounds__(WT) k_h_sv_t(HView h, int l, int parity, const double* x, int64_t ldx, int nrhs,
+                                               double* part) {
+  __shared__ double red[WT / 32][HMAX_RANK];
+  const int node = blockIdx.y, c = 2 * node + parity, k = h.k;
+  const int64_t sl = h.s(l);
+  const int nch = (int)((sl + MV_CHUNK - 1) / MV_CHUNK);
+  const int64_t i0 = (int64_t)blockIdx.x * MV_CHUNK, i1 = min(sl, i0 + MV_CHUNK);
+  const double* Vb = h.v(l, c);
+  const int64_t col0 = (int64_t)(c ^ 1) * sl;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int q = 0; q < nrhs; ++q) {
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = i0 + wid; i < i1; i += WT / 32) {
+      const double xv = x[col0 + i + q * ldx];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int rr = lane + 32 * t;
+        if (rr < k) acc[t] += Vb[rr + i * k] * xv;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+      if (lane + 32 * t < k) red[wid][lane + 32 * t] = acc[t];
+    __syncthreads();
+    for (int rr = threadIdx.x; rr < k; rr += WT) {
+      double v = 0.0;
+      for (int w = 0; w < WT / 32; ++w) v += red[w][rr];
+      part[(((int64_t)node * nch + blockIdx.x) * nrhs + q) * k + rr] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// x(rows of c) -= WZ_c S_c sum_chunks T[node][chunk], c = 2 node + parity
+// (grid: row tiles x nodes); hw.U addresses the W / Z slab, hw.S the factor's S.
+__global__ void __launch_bounds__(WT) k_h_sv_u(HView hw, int l, int parity, int nrhs, const double* part, double* x,
+                                               int64_t ldx) {
+  __shared__ double t1[HMAX_RANK];
+  __shared__ double t2[HMAX_RANK];
+  const int node = blockIdx.y, c = 2 * node + parity, k = hw.k;
+  const int64_t sl = hw.s(l);
+  const int nch = (int)((sl + MV_CHUNK - 1) / MV_CHUNK);
+  const double* Wb = hw.u(l, c);
+  const double* Sb = hw.sm(l, c);
+  const int64_t row0 = (int64_t)c * sl;
+  const int64_t i = (int64_t)blockIdx.x * WT + threadIdx.x;
+  for (int q = 0; q < nrhs; ++q) {
+    for (int rr = threadIdx.x; rr < k; rr += WT) {
+      double v = 0.0;
+      for (int g = 0; g < nch; ++g) v += part[(((int64_t)node * nch + g) * nrhs + q) * k + rr];
+      t1[rr] = v;
+    }
+    __syncthreads();
+    for (int rr = threadIdx.x; rr < k; rr += WT) {
+      double v = 0.0;
+      for (int t = 0; t < k; ++t) v += Sb[rr + t * k] * t1[t];
+      t2[rr] = v;
+    }
+    __syncthreads();
+    if (i < sl) {
+      double v = 0.0;
+      for (int t = 0; t < k; ++t) v += Wb[i + (int64_t)t * sl] * t2[t];
+      x[row0 + i + q * ldx] -= v;
+    }
+    __syncthreads();
+  }
+}
+
 // y_p = D_p x_p for every leaf (grid: leaves), nrhs columns.
 __global__ void __launch_bounds__(WT) k_h_mv_leaf(int b, const double* D, const double* x, int64_t ldx, double* y,
                                                   int64_t ldy, int nrhs) {
@@ -480,8 +588,6 @@ __global__ void __launch_bounds__(WT) k_h_mv_leaf(int b, const double* D, const 
     __syncthreads();
   }
 }
-
-constexpr int MV_CHUNK = 1024;
 
 // Partials T[c][chunk] (k x nrhs) = V_c(:, chunk) x(cols of c, chunk) of one
 // level (grid: chunks x blocks).
@@ -621,6 +727,9 @@ struct frank_hodlr {
   std::vector<cudaStream_t> ls;     // [L + 1] one stream per level for the LowRank additions
   std::vector<cudaEvent_t> lev;     // [L + 1] last addition enqueued on level j's stream
   cudaEvent_t ev_fork = nullptr, ev_core = nullptr;
+  double* WZ = nullptr;             // per node: W (lower block's slot) and Z (upper block's slot), U-shaped
+  cudaStream_t ps = nullptr;        // their walks, beside the factorization
+  cudaEvent_t ev_pre = nullptr, ev_ps = nullptr;
   ::frank::ops::LrAddTask* tasks_d = nullptr;   // every update's additions, in launch order
   std::vector<::frank::ops::LrAddTask> tasks_h;
   int64_t ntasks_cap = 0;
@@ -768,6 +877,22 @@ void enqueue_update(frank_hodlr* h, int lr, int cr, const double* Ux, const doub
   }
 }
 
+// WZ(l, c) <- the substitution (mode 0: L with pivots, 2: U) of cluster
+// (l, c)'s subtree applied to the U factor of block (l, c), on stream ps after
+// everything enqueued so far on s.
+void enqueue_precompute(frank_hodlr* h, int l, int c, int mode, cudaStream_t s) {
+  const int k = h->k;
+  const int64_t sl = s_of(h, l);
+  cudaEventRecord(h->ev_pre, s);
+  cudaStreamWaitEvent(h->ps, h->ev_pre, 0);
+  cudaMemcpyAsync(h->WZ + u_off(h, l, c), h->U + u_off(h, l, c), sizeof(double) * sl * k, cudaMemcpyDeviceToDevice,
+                  h->ps);
+  hk::Walk j0{mode, l, c, k, h->WZ + u_off(h, l, c), 1, sl}, none{0, 0, 0, 0, nullptr, 1, 1};
+  hk::k_h_walk<<<dim3((k + hk::WCW - 1) / hk::WCW, 1), hk::WWT, hk::WALK_SMEM, h->ps>>>(view(h, true),
+                                                                                       leaf_factors(h), j0, none);
+  ++h->launches;
+}
+
 void enqueue_node(frank_hodlr* h, int l, int c, cudaStream_t s) {
   if (l == h->L) {
     enqueue_leaf(h, c, s);
@@ -785,6 +910,8 @@ void enqueue_node(frank_hodlr* h, int l, int c, cudaStream_t s) {
   hk::Walk j1{1, l + 1, 2 * c, k, h->V + u_off(h, l + 1, lo), k, 1};
   hk::k_h_walk<<<dim3((k + hk::WCW - 1) / hk::WCW, 2), hk::WWT, hk::WALK_SMEM, s>>>(view(h, true), leaf_factors(h),
                                                                                    j0, j1);
+  // for the level-parallel solve, beside the factorization: Z = U_left^{-1} U_up
+  enqueue_precompute(h, l + 1, up, 2, s);
   // S' = -(S_low V_low)(U_up S_up), one k x k slot per internal node
   double* Sp = h->Sp + ((int64_t)(1 << l) - 1 + c) * k * k;
   const int grid = (int)std::min<int64_t>(CORE_GRID, (sc + 511) / 512);
@@ -795,6 +922,8 @@ void enqueue_node(frank_hodlr* h, int l, int c, cudaStream_t s) {
   h->launches += 2;
   enqueue_update(h, l + 1, lo, h->U + u_off(h, l + 1, lo), h->V + u_off(h, l + 1, up), Sp, s);
   enqueue_node(h, l + 1, 2 * c + 1, s);
+  // W = M_right(U_low), once the right child is factored
+  enqueue_precompute(h, l + 1, lo, 0, s);
 }
 
 int enqueue_factor(frank_hodlr* h, cudaStream_t s) {
@@ -807,6 +936,7 @@ int enqueue_factor(frank_hodlr* h, cudaStream_t s) {
   h->launches = 0;
   h->tasks_h.clear();
   H_TRY(cudaEventRecord(h->ev_fork, s));
+  H_TRY(cudaStreamWaitEvent(h->ps, h->ev_fork, 0));
   for (int j = 1; j <= h->L; ++j) {
     H_TRY(cudaStreamWaitEvent(h->ls[j], h->ev_fork, 0));
     H_TRY(cudaEventRecord(h->lev[j], h->ls[j]));
@@ -816,6 +946,8 @@ int enqueue_factor(frank_hodlr* h, cudaStream_t s) {
     H_TRY(cudaEventRecord(h->lev[j], h->ls[j]));
     H_TRY(cudaStreamWaitEvent(s, h->lev[j], 0));
   }
+  H_TRY(cudaEventRecord(h->ev_ps, h->ps));
+  H_TRY(cudaStreamWaitEvent(s, h->ev_ps, 0));
   H_TRY(cudaGetLastError());
   return FRANK_OK;
 }
@@ -844,6 +976,10 @@ void free_plan(frank_hodlr* h) {
   for (cudaEvent_t x : h->lev) if (x) cudaEventDestroy(x);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_core) cudaEventDestroy(h->ev_core);
+  if (h->ev_pre) cudaEventDestroy(h->ev_pre);
+  if (h->ev_ps) cudaEventDestroy(h->ev_ps);
+  if (h->ps) cudaStreamDestroy(h->ps);
+  if (h->WZ) cudaFree(h->WZ);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
 }
@@ -891,13 +1027,27 @@ int enqueue_matvec(frank_hodlr* h, const double* x, int64_t ldx, double* y, int6
 }
 
 int enqueue_solve(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, cudaStream_t s) {
+  int rc = ensure_mv(h, nrhs);
+  if (rc) return rc;
   const hk::HView v = view(h, true);
+  hk::HView vw = v;
+  vw.U = h->WZ;
   const hk::LeafFactors f = leaf_factors(h);
-  const unsigned g = (unsigned)((nrhs + hk::WCW - 1) / hk::WCW);
-  hk::Walk fw{0, 0, 0, nrhs, d_b, 1, ldb}, none{0, 0, 0, 0, nullptr, 1, 1};
-  hk::k_h_walk<<<dim3(g, 1), hk::WWT, hk::WALK_SMEM, s>>>(v, f, fw, none);
-  hk::Walk bw{2, 0, 0, nrhs, d_b, 1, ldb};
-  hk::k_h_walk<<<dim3(g, 1), hk::WWT, hk::WALK_SMEM, s>>>(v, f, bw, none);
+  const dim3 gleaf(h->P, (nrhs + hk::WCW - 1) / hk::WCW);
+  for (int pass = 0; pass < 2; ++pass) {
+    // forward: leaves with L and pivots, then lower blocks (odd); backward:
+    // leaves with U, then upper blocks (even)
+    hk::k_h_leaf_apply<<<gleaf, hk::WT, 0, s>>>(h->b, pass == 0 ? 0 : 2, f, d_b, ldb, nrhs);
+    const int parity = pass == 0 ? 1 : 0;
+    for (int l = h->L; l >= 1; --l) {
+      const int64_t sl = s_of(h, l);
+      const int nch = (int)((sl + hk::MV_CHUNK - 1) / hk::MV_CHUNK);
+      const int nodes = 1 << (l - 1);
+      hk::k_h_sv_t<<<dim3(nch, nodes), hk::WT, 0, s>>>(v, l, parity, d_b, ldb, nrhs, h->mv_part);
+      hk::k_h_sv_u<<<dim3((unsigned)((sl + hk::WT - 1) / hk::WT), nodes), hk::WT, 0, s>>>(vw, l, parity, nrhs,
+                                                                                           h->mv_part, d_b, ldb);
+    }
+  }
   H_TRY(cudaGetLastError());
   return FRANK_OK;
 }
@@ -962,6 +1112,10 @@ int frank_hodlr_create(int64_t n, int leaf, int rank, frank_hodlr** out) {
   }
   A(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   A(cudaEventCreateWithFlags(&h->ev_core, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&h->ev_pre, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&h->ev_ps, cudaEventDisableTiming));
+  A(cudaStreamCreateWithFlags(&h->ps, cudaStreamNonBlocking));
+  A(dalloc(&h->WZ, (size_t)nk));
   h->lr_shm = ::frank::ops::lr_add_shm_bytes(rank, rank);
   A(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
   A(cudaEventCreate(&h->e0));
