@@ -129,6 +129,7 @@ SIGNATURES = {
     "frank_hodlr_build_kernel": (C.c_int, [_vp, C.c_int, _dp, C.c_int, _dp, _vp]),
     "frank_hodlr_getrf": (C.c_int, [_vp, _vp]),
     "frank_hodlr_solve_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int, _vp]),
+    "frank_hodlr_trsm_device": (C.c_int, [_vp, C.c_int, C.c_void_p, C.c_int64, C.c_int, _vp]),
     "frank_hodlr_matvec_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, _vp]),
     "frank_hodlr_refine_device": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int,
                                             C.c_double, C.c_int, _ip, _dp, _vp]),

@@ -1026,7 +1026,8 @@ int enqueue_matvec(frank_hodlr* h, const double* x, int64_t ldx, double* y, int6
   return FRANK_OK;
 }
 
-int enqueue_solve(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, cudaStream_t s) {
+// passes: 1 = forward (L with the pivots), 2 = backward (U), 3 = both.
+int enqueue_solve(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, cudaStream_t s, int passes = 3) {
   int rc = ensure_mv(h, nrhs);
   if (rc) return rc;
   const hk::HView v = view(h, true);
@@ -1035,6 +1036,7 @@ int enqueue_solve(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, cudaStream
   const hk::LeafFactors f = leaf_factors(h);
   const dim3 gleaf(h->P, (nrhs + hk::WCW - 1) / hk::WCW);
   for (int pass = 0; pass < 2; ++pass) {
+    if (!(passes & (1 << pass))) continue;
     // forward: leaves with L and pivots, then lower blocks (odd); backward:
     // leaves with U, then upper blocks (even)
     hk::k_h_leaf_apply<<<gleaf, hk::WT, 0, s>>>(h->b, pass == 0 ? 0 : 2, f, d_b, ldb, nrhs);
@@ -1357,6 +1359,18 @@ int frank_hodlr_solve_device(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs,
   if (!h->factored) return hfail(FRANK_ERR_STATE, "solve before getrf");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = enqueue_solve(h, d_b, ldb, nrhs, s);
+  if (rc) return rc;
+  H_TRY(cudaStreamSynchronize(s));
+  return FRANK_OK;
+}
+
+int frank_hodlr_trsm_device(frank_hodlr* h, int uplo, double* d_b, int64_t ldb, int nrhs, void* stream) {
+  if (!h || !d_b) return hfail(FRANK_ERR_INVALID, "null argument");
+  if (nrhs < 1 || ldb < h->n || (uplo != FRANK_LOWER && uplo != FRANK_UPPER))
+    return hfail(FRANK_ERR_INVALID, "bad right-hand sides or triangle");
+  if (!h->factored) return hfail(FRANK_ERR_STATE, "trsm before getrf");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = enqueue_solve(h, d_b, ldb, nrhs, s, uplo == FRANK_LOWER ? 1 : 2);
   if (rc) return rc;
   H_TRY(cudaStreamSynchronize(s));
   return FRANK_OK;

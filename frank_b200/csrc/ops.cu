@@ -357,6 +357,25 @@ __global__ void __launch_bounds__(OT) k_op_rid(int m, int n, int s, int k, Mat A
 // else ka.  fast (fixed rank, Ua and Va^T orthonormal): the projections
 // Zu = Ua^T Ub, Zv = Va Vb^T, QR of the remainders only, core
 // [I Zu; 0 Ru] blockdiag(Sa, Sb) [I Zv; 0 Rv]^T.
+// Optional phase counters of the LowRank addition (build with
+// -DFRANK_LRA_TIMING; off by default): [0] operands and projections,
+// [1] QR of the remainders, [2] core and its SVD, [3] new bases, [4] count.
+#ifdef FRANK_LRA_TIMING
+__device__ unsigned long long g_lra_cycles[8];
+#define LRA_MARK(k)                                                                          \
+  do {                                                                                       \
+    if (threadIdx.x == 0) {                                                                  \
+      const long long _t = clock64();                                                        \
+      atomicAdd(&g_lra_cycles[(k)], (unsigned long long)(_t - _lra_t0));                     \
+      _lra_t0 = _t;                                                                          \
+    }                                                                                        \
+  } while (0)
+#define LRA_BEGIN() long long _lra_t0 = clock64()
+#else
+#define LRA_MARK(k) do {} while (0)
+#define LRA_BEGIN() do {} while (0)
+#endif
+
 FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* ua_out, int64_t ldua, double* sa_out,
                          int64_t ldsa, double* va_out, int64_t ldva, int* ka_io, const double* ub, int64_t ldub,
                          const double* sb, int64_t ldsb, const double* vb, int64_t ldvb, int kb, double* X, int* err,
@@ -379,6 +398,7 @@ FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* u
   double* sc = T + (int64_t)max(m, n) * kt;     // svd scratch (2 kt + 2) kt
   const double *ua = ua_out, *sa = sa_out, *va = va_out;
   struct LD { int64_t ld; } Ua{ldua}, Sa{ldsa}, Va{ldva}, Ub{ldub}, Sb{ldsb}, Vb{ldvb};
+  LRA_BEGIN();
   const bool use_fast = fast && eps == 0.0 && kt <= m && kt <= n;
   int mu, mv;
   if (!use_fast) {
@@ -427,8 +447,10 @@ FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* u
                          gsm);
     cta_gemm<double, OT>(n, kb, ka, -1.0, Y, n, false, Rv + (int64_t)ka * kt, kt, false, 1.0, Y + (int64_t)ka * n, n,
                          gsm);
+    LRA_MARK(0);
     cta_householder_qr(m, kb, X + (int64_t)ka * m, m, tu, red);
     cta_householder_qr(n, kb, Y + (int64_t)ka * n, n, tv, red);
+    LRA_MARK(1);
     for (int64_t e = threadIdx.x; e < (int64_t)kt * kt; e += blockDim.x) {
       const int r = e % kt, c = e / kt;
       if (c < ka) { Rc[e] = r == c ? 1.0 : 0.0; Rv[e] = r == c ? 1.0 : 0.0; }
@@ -446,6 +468,7 @@ FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* u
   }
   if (!cta_svd(mu, mv, M, mu, Um, mu, sv, Vmt, min(mu, mv), sc, &flag, shm, shm_cap) && threadIdx.x == 0)
     atomicAdd(err + OPS_ERR_JACOBI, 1);
+  LRA_MARK(2);
   const int nsv = min(mu, mv);
   if (threadIdx.x == 0) {
     int r;
@@ -509,6 +532,10 @@ FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* u
     }
     __syncthreads();
   }
+  LRA_MARK(3);
+#ifdef FRANK_LRA_TIMING
+  if (threadIdx.x == 0) atomicAdd(&g_lra_cycles[4], 1ull);
+#endif
   double* sp = sa_out;
   for (int64_t e = threadIdx.x; e < (int64_t)r * r; e += blockDim.x) {
     const int i = e % r, c = e / r;
@@ -937,5 +964,12 @@ int frank_lowrank_add_batched(int m, int n, int count, int kmax, const char* lra
                                      Mat{const_cast<double*>(d_vb), ldvb, svb}, d_kb, sc, ws, err, 0);
   });
 }
+
+#ifdef FRANK_LRA_TIMING
+int frank_debug_lra_cycles(unsigned long long* out) {
+  OPS_TRY(cudaMemcpyFromSymbol(out, g_lra_cycles, sizeof(unsigned long long) * 8));
+  return FRANK_OK;
+}
+#endif
 
 }  // extern "C"

@@ -125,10 +125,20 @@ class HMatrix:
 
     # host arrays (n x nrhs), through a device buffer
     def solve(self, b: np.ndarray) -> np.ndarray:
-        bb = np.asfortranarray(np.asarray(b, dtype=np.float64).reshape(self.n, -1))
+        bb = np.array(np.asarray(b, dtype=np.float64).reshape(self.n, -1), order="F", copy=True)
         d = _DeviceBuffer(bb.size)
         d.put(bb)
         check(lib().frank_hodlr_solve_device(self._h, d.ptr, self.n, bb.shape[1], None), "frank_hodlr_solve_device")
+        d.get(bb)
+        return bb if np.ndim(b) == 2 else bb[:, 0]
+
+    def trsm(self, b: np.ndarray, lower: bool) -> np.ndarray:
+        """trsm(L, b, Lower) (lower=True: b <- L^{-1} P b) or trsm(U, b, Upper)."""
+        bb = np.array(np.asarray(b, dtype=np.float64).reshape(self.n, -1), order="F", copy=True)
+        d = _DeviceBuffer(bb.size)
+        d.put(bb)
+        check(lib().frank_hodlr_trsm_device(self._h, 0 if lower else 1, d.ptr, self.n, bb.shape[1], None),
+              "frank_hodlr_trsm_device")
         d.get(bb)
         return bb if np.ndim(b) == 2 else bb[:, 0]
 

@@ -494,6 +494,9 @@ int frank_hodlr_getrf(frank_hodlr* h, void* stream);
 /* b <- (L U)^{-1} P b in place: trsm(L, b, Lower) then trsm(U, b, Upper)
  * (examples/h_lu.cpp:45-48); device buffer n x nrhs, ld ldb. */
 int frank_hodlr_solve_device(frank_hodlr* h, double* d_b, int64_t ldb, int nrhs, void* stream);
+/* One of the two: uplo FRANK_LOWER: b <- L^{-1} P b (trsm(L, b, Mode::Lower));
+ * FRANK_UPPER: b <- U^{-1} b (trsm(U, b, Mode::Upper)); in either order. */
+int frank_hodlr_trsm_device(frank_hodlr* h, int uplo, double* d_b, int64_t ldb, int nrhs, void* stream);
 /* y = A_H x (FP64; gemm(H, x, y) over the leaves and every LowRank block). */
 int frank_hodlr_matvec_device(frank_hodlr* h, const double* d_x, int64_t ldx, double* d_y, int64_t ldy, int nrhs,
                               void* stream);

@@ -116,6 +116,14 @@ def test_hodlr_solve_matches_oracle(n, leaf, rank):
     err, err_ref = fo.l2_error(x, sol), fo.l2_error(x, sol_ref)
     assert err <= 10.0 * err_ref + 1e-13, (err, err_ref)
     assert _rel(sol, sol_ref) < 1e-8
+    # the two triangular solves one at a time, as trsm(L, b, Lower) and
+    # trsm(U, b, Upper) (trsm.cpp:40-90 through the oracle's recursion)
+    y = M.trsm(b, lower=True)
+    y_ref = fo.trsm(L, np.array(b_ref, copy=True), upper=False, left=True)
+    assert _rel(y, y_ref) < 1e-8
+    z = M.trsm(y, lower=False)
+    z_ref = fo.trsm(U, np.array(y_ref, copy=True), upper=True, left=True)
+    assert _rel(z, z_ref) < 1e-8
     M.close()
 
 
