@@ -119,6 +119,47 @@ FRANK_D bool cta_svd(int m, int n, const double* a, int64_t lda, double* U, int6
   return ok;
 }
 
+// SVD of a square a (n x n, lda) preconditioned by column-pivoted QR
+// (Drmac and Veselic, "New fast and accurate Jacobi SVD algorithm", 2008):
+// a P = Q R, one-sided Jacobi on the columns of R^T with the rotations V
+// accumulated, R^T V = Y; then a = (Q V) diag(sigma) (P Y diag(1/sigma))^T.
+// The pivoted R is graded, so the sweeps converge in a few passes.  All of it
+// in shared memory shm (3 n^2 doubles); sc: 4 n doubles + 2 n ints (global).
+// Outputs as cta_svd.
+FRANK_D bool cta_svd_pqr(int n, const double* a, int64_t lda, double* U, int64_t ldu, double* s, double* Vt,
+                         int64_t ldvt, double* sc, double* shm, int* flag, double* red, int* redi) {
+  double* W = shm;                                  // n x n: R above, reflectors below
+  double* G = shm + (int64_t)n * n;                 // 2n x n (ld 2n): [R^T; I], rotated
+  double* tau = sc;
+  double* cn = tau + n;
+  double* pn = cn + n;
+  double* sig = pn + n;
+  int* jpvt = reinterpret_cast<int*>(sig + n);
+  int* ord = jpvt + n;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) W[e] = a[e % n + (int64_t)(e / n) * lda];
+  __syncthreads();
+  cta_truncated_geqp3(n, n, W, n, -1.0, n, tau, cn, pn, jpvt, red, redi);
+  __syncthreads();
+  const int ldg = 2 * n;
+  for (int e = threadIdx.x; e < ldg * n; e += blockDim.x) {
+    const int r = e % ldg, c = e / ldg;
+    G[e] = r < n ? (c <= r ? W[c + r * n] : 0.0) : (r - n == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const bool ok = jacobi_svd(n, n, G, sig, ord, flag);
+  cta_apply_q(n, n, W, n, tau, n, G + n, ldg);     // rows n..2n-1 become Q V
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e % n, j = e / n, c = ord[j];
+    U[r + (int64_t)j * ldu] = G[n + r + c * ldg];
+    const double sv = sig[c];
+    Vt[j + (int64_t)jpvt[r] * ldvt] = sv > 0.0 ? G[r + c * ldg] / sv : 0.0;
+  }
+  for (int j = threadIdx.x; j < n; j += blockDim.x) s[j] = sig[ord[j]];
+  __syncthreads();
+  return ok;
+}
+
 // The first k steps of the column-pivoted QR of W (m x n, ld m) in place;
 // jpvt (n): original column at pivoted position.  geqp3
 // (operations/LAPACK/geqp3.cpp:36-69: LAPACKE_dgeqp3) pivots greedily on the
@@ -382,6 +423,7 @@ FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* u
                          double* shm, int64_t shm_cap) {
   __shared__ double gsm[GSM];
   __shared__ double red[32];
+  __shared__ int redi[32];
   __shared__ int flag, s_rank;
   const int ka = *ka_io;
   const int kt = ka + kb;
@@ -466,8 +508,10 @@ FRANK_D void lr_add_body(int m, int n, int kmax, int fast, double eps, double* u
                          T + (int64_t)ka * kt, kt, gsm);
     cta_gemm<double, OT>(kt, kt, kt, 1.0, T, kt, false, Rv, kt, true, 0.0, M, kt, gsm);
   }
-  if (!cta_svd(mu, mv, M, mu, Um, mu, sv, Vmt, min(mu, mv), sc, &flag, shm, shm_cap) && threadIdx.x == 0)
-    atomicAdd(err + OPS_ERR_JACOBI, 1);
+  const bool svd_ok = (mu == mv && shm && 3 * (int64_t)mu * mu <= shm_cap)
+                          ? cta_svd_pqr(mu, M, mu, Um, mu, sv, Vmt, mu, sc, shm, &flag, red, redi)
+                          : cta_svd(mu, mv, M, mu, Um, mu, sv, Vmt, min(mu, mv), sc, &flag, shm, shm_cap);
+  if (!svd_ok && threadIdx.x == 0) atomicAdd(err + OPS_ERR_JACOBI, 1);
   LRA_MARK(2);
   const int nsv = min(mu, mv);
   if (threadIdx.x == 0) {
@@ -711,10 +755,11 @@ void launch_svd(cudaStream_t s, int m, int n, int count, const double* a, int64_
                                 Mat{vt, ldvt, svt}, scratch, ws, err);
 }
 
-// Shared memory (bytes) for the core SVD of an addition of ranks ka + kb,
-// or 0 when it does not fit beside the kernel's static arrays.
+// Shared memory (bytes) for the core SVD of an addition of ranks ka + kb
+// (the pivoted-QR-preconditioned Jacobi: 3 kt^2 doubles), or 0 when it does
+// not fit beside the kernel's static arrays.
 int lr_add_shm_bytes(int ka, int kb) {
-  const int64_t kt = ka + kb, b = (2 * kt) * kt * (int64_t)sizeof(double);
+  const int64_t kt = ka + kb, b = (3 * kt) * kt * (int64_t)sizeof(double);
   return b <= 160 * 1024 ? (int)b : 0;
 }
 
