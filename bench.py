@@ -661,16 +661,16 @@ def workload_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
-def workload_hlu(args):
-    """Multi-level H-LU: Laplace-3D 1/(r+1e-3) on N = 131072 (--hlu-n)
-    Morton-ordered unit-cube points (seed 7), binary cluster tree with weak
-    admissibility, leaves of 256, every off-diagonal block rank 32 (rsvd),
-    FP64 factor, FP64 refinement of 8 RHS (seed 8) against A_H to 1e-10.  A
-    step is getrf + refine; construction is timed apart.  Prints one JSON
-    line."""
+def run_hlu(n, steps, warmup):
+    """Multi-level H-LU: Laplace-3D 1/(r+1e-3) on N = n Morton-ordered
+    unit-cube points (seed 7), binary cluster tree with weak admissibility,
+    leaves of 256, every off-diagonal block rank 32 (rsvd), FP64 factor, FP64
+    refinement of 8 RHS (seed 8) against A_H to 1e-10.  A step is getrf +
+    refine (wall clock around synchronised calls; the getrf's device time from
+    CUDA events beside it); construction is timed apart.  Returns a dict."""
     import torch
     from frank_b200 import HMatrix
-    n, leaf, rank, nrhs = args.hlu_n, 256, 32, 8
+    leaf, rank, nrhs = 256, 32, 8
     pts = make_points(n, 3, 7, 10)
     M = HMatrix(n, leaf, rank)
     torch.cuda.synchronize(); t0 = time.perf_counter()
@@ -680,10 +680,10 @@ def workload_hlu(args):
     b = torch.tensor(MT19937_64(8).normal(n * nrhs).reshape(nrhs, n), device="cuda").t()
     X = torch.zeros((nrhs, n), dtype=torch.float64, device="cuda").t()
     its = res = None
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         M.getrf(); M.refine_device(b.data_ptr(), X.data_ptr(), nrhs, tol=1e-10, maxit=50)
     times, tf = [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize(); t0 = time.perf_counter()
         M.getrf()
         torch.cuda.synchronize(); t1 = time.perf_counter()
@@ -694,14 +694,19 @@ def workload_hlu(args):
     M.matvec_device(X.data_ptr(), Y.data_ptr(), nrhs)
     rel = ((b - Y).norm(dim=0) / b.norm(dim=0)).max().item()
     st = M.stats()
-    print(json.dumps({"workload": "hlu: laplace3d N=%d leaf=256 rank=32 weak admissibility, FP64, 8 rhs, tol 1e-10" % n,
-                      "metric": "time to 1e-10 (getrf + refine)", "value": statistics.median(times), "unit": "s",
-                      "getrf_s": statistics.median(tf), "getrf_device_ms": st["factor_ms"],
-                      "refine_s": statistics.median(times) - statistics.median(tf), "iterations": its,
-                      "residual": res, "residual_recomputed": rel, "launches_per_getrf": st["launches"],
-                      "levels": M.levels, "build_s": t_build, "steps": args.steps, "warmup": args.warmup}),
-          flush=True)
+    out = {"workload": "hlu: laplace3d N=%d leaf=256 rank=32 weak admissibility, FP64, 8 rhs, tol 1e-10" % n,
+           "metric": "time to 1e-10 (getrf + refine)", "value": statistics.median(times), "unit": "s",
+           "getrf_s": statistics.median(tf), "getrf_device_ms": st["factor_ms"],
+           "refine_s": statistics.median(times) - statistics.median(tf), "iterations": its,
+           "residual": res, "residual_recomputed": rel, "launches_per_getrf": st["launches"],
+           "levels": M.levels, "build_s": t_build, "steps": steps, "warmup": warmup}
     M.close()
+    return out
+
+
+def workload_hlu(args):
+    """The multi-level H-LU workload (run_hlu) at --hlu-n; prints one JSON line."""
+    print(json.dumps(run_hlu(args.hlu_n, args.steps, args.warmup)), flush=True)
 
 
 def main():
@@ -718,6 +723,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-hlu", action="store_true", help="leave out the multi-level H-LU key of the bench line")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)
@@ -791,6 +797,12 @@ def main():
             "clocks": mx["clocks"],
         }
         line["sample"] = dict(workload=SAMPLE_DESC, unit="s", **sample_ours)
+        if world == 1 and not args.no_hlu:
+            # the multi-level H-LU configuration beside the headline (its own timing)
+            try:
+                line["hlu"] = run_hlu(131072, args.steps, max(args.warmup, 3))
+            except Exception as exc:  # reported, never silently dropped
+                line["hlu"] = {"error": str(exc)}
         if not args.no_cpu_baseline:
             cores = os.cpu_count()
             t, info = run_reference_sample(3, 1, cores)
