@@ -82,7 +82,7 @@ CPP_LIB = os.path.join(LIBDIR, "libfrank_b200_cpp.so")
 def build_cpp(force: bool = False) -> str:
     """The C++ layer (namespace FRANK over the C ABI) as libfrank_b200_cpp.so,
     linked against libfrank_b200.so next to it."""
-    lib = build(force=force)
+    lib = build()
     srcs = [os.path.join(CPP_DIR, "frank.cpp")]
     deps = srcs + [os.path.join(CPP_DIR, "include", "frank_b200", f) for f in ("FRANK.hpp", "multimethod.hpp")]
     deps.append(os.path.join(HERE, "..", "include", "frank_b200.h"))
